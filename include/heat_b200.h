@@ -1,0 +1,189 @@
+/* heat_b200.h -- C ABI of the B200 transient-heat PCG library (libheat_b200.so).
+ *
+ * One opaque solver handle per problem instance (grid, material field, time
+ * step, operator options).  Every entry point returns an hs_status; nothing
+ * aborts the process.  The CLI (hs_cli_main) maps the codes onto the exit
+ * codes of the reference solver.
+ *
+ * The reference, src/heat_solver_het.cu, has no library API: its operator is
+ * a C++ class (HeatOperator, het.cu:618-989) plus a free PCG function
+ * (pcg_solve, het.cu:994-1039) driven by a CLI (main, het.cu:1355-1629).
+ * Each declaration below names the reference code it replaces.
+ *
+ * Vector arguments marked "device" are device pointers to (N+1)^3 float64
+ * node values in the reference's node order n = ix*(N+1)^2 + iy*(N+1) + iz
+ * (het.cu:202-205).  Element fields are N^3 float64 in element order
+ * e = ix*N^2 + iy*N + iz (het.cu:289-291, scripts/gen_field.py:5-6).
+ *
+ * Threading: a handle is used by one host thread at a time; handles are
+ * independent and each owns its own CUDA stream.
+ */
+#ifndef HEAT_B200_H
+#define HEAT_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HS_API_VERSION 1
+
+typedef struct hs_solver hs_solver;
+
+typedef enum hs_status {
+    HS_OK = 0,
+    HS_ERR_ARG = 1,      /* bad argument, bad field value; reference: MPI_Abort(.., 1) */
+    HS_ERR_MATRIX = 2,   /* reference-matrix self-check failed; reference: MPI_Abort(.., 2), het.cu:705 */
+    HS_ERR_IO = 3,       /* missing or short field file, unwritable output (exit code 1 in the CLI) */
+    HS_ERR_CUDA = 4,     /* CUDA error or no device (exit code 1 in the CLI) */
+    HS_ERR_STATE = 5     /* call not valid for this handle's options */
+} hs_status;
+
+/* element operator form (--kernel) */
+enum {
+    HS_KERNEL_FAST = 0,   /* rhoc*M^ + dt*k*K^ with the Gauss-built 8x8 matrices, het.cu:340-349 */
+    HS_KERNEL_GAUSS = 1,  /* 2x2x2 Gauss integration per call, het.cu:310-338 */
+    HS_KERNEL_WHT = 2     /* same element matrix through its exact tensor-product
+                             (Walsh-Hadamard) structure; no reference counterpart */
+};
+/* scatter (--scatter) */
+enum { HS_SCATTER_ATOMIC = 0, HS_SCATTER_COLORED = 1 };
+/* fault-injection levels (--fi LEVEL ...) */
+enum {
+    HS_FI_NONE = 0,
+    HS_FI_G = 1,   /* T[target % Nn] before the RHS of the step, het.cu:1130-1135 */
+    HS_FI_R = 2,   /* ye[0] of element `target` in the step's first matvec, het.cu:369-374 */
+    HS_FI_H = 3,   /* host halo buffer; needs >= 2 ranks, rejected here (het.cu:1419-1422) */
+    HS_FI_P = 5,   /* PCG search direction p[target % Nn] at loop iteration `iter` (new) */
+    HS_FI_RV = 6,  /* PCG residual r[target % Nn] after its update at iteration `iter` (new) */
+    HS_FI_AP = 7   /* operator output Ap[target % Nn] at iteration `iter` (new) */
+};
+
+/* Solver options; hs_default_options fills the reference defaults
+ * (het.cu:1385-1391: kernel fast, scatter atomic, tol 1e-8, 500 iterations). */
+typedef struct hs_options {
+    int N;              /* elements per axis on [0,1]^3 */
+    double dt;          /* implicit-Euler step */
+    int kernel;         /* HS_KERNEL_* */
+    int scatter;        /* HS_SCATTER_* */
+    int detect;         /* D1/D2/D3 detectors (--detect) */
+    int verify;         /* eigenmode check mode: source off (--verify) */
+    int no_source;      /* --no-source */
+    int ic_mode;        /* 0 zero, 1 Gaussian bump (--ic) */
+    double ic_sigma;    /* Gaussian IC width, reference 0.1 (het.cu:566) (--ic-sigma, new) */
+    double rtol;        /* PCG relative tolerance, reference 1e-8 (het.cu:1162) (--rtol, new) */
+    int max_iter;       /* PCG iteration cap, reference 500 */
+    int device;         /* CUDA device ordinal */
+} hs_options;
+
+typedef struct hs_fi_spec {
+    int level;          /* HS_FI_* */
+    int step;           /* time step at which it fires */
+    long long target;   /* node (G, P, RV, AP: taken modulo Nn) or element (R) index */
+    int bit;            /* 0..63, XOR on the IEEE-754 word */
+    int iter;           /* PCG loop iteration (P, RV, AP) */
+    int rank;           /* --fi-rank; only 0 is valid on one device */
+} hs_fi_spec;
+
+/* per-step record of one trajectory (RunResult, het.cu:1082-1096) */
+typedef struct hs_step_record {
+    int cg_iters;
+    int snap;           /* 1 if the step was a snapshot step */
+    double d1, d2, tmin, tmax;   /* detectors (0 when detect is off) */
+    double E, spread;   /* vs the reference trajectory at snapshot steps, else -1 / 0 */
+    double solve_ms;    /* build_rhs + PCG (+ reprojection) device time of the step */
+} hs_step_record;
+
+/* canonical reduction tile: planes (x), rows (y), columns (z), threads */
+typedef struct hs_layout_info { int cx, ty, tz, rt, bpt; } hs_layout_info;
+
+void        hs_default_options(hs_options* opt);
+const char* hs_last_error(void);               /* message of the last failing call on this thread */
+int         hs_api_version(void);
+void        hs_get_layout(hs_layout_info* out);
+
+/* Read <prefix>_k.bin and <prefix>_rhoc.bin (N^3 float64 each) into host
+ * buffers; rejects short files and non-positive/NaN values
+ * (HeatOperator::load_fields, het.cu:711-753). */
+hs_status hs_load_fields(const char* prefix, int N, double* k_out, double* rhoc_out);
+
+/* Build the operator: reference matrices + self-check, Jacobi diagonal,
+ * source vector, ABFT weights (HeatOperator::setup, het.cu:756-816, 940-953).
+ * k/rhoc are host arrays of N^3 values. */
+hs_status hs_create(const hs_options* opt, const double* k_host, const double* rhoc_host, hs_solver** out);
+void      hs_destroy(hs_solver* s);
+long long hs_num_nodes(const hs_solver* s);
+/* kmin, kmax, rhocmin, rhocmax and the five reference-matrix check errors */
+hs_status hs_field_stats(const hs_solver* s, double out9[9]);
+
+/* y = (M + dt_eff K) x [+ Dirichlet projection] (apply_operator, het.cu:885-921).
+ * allow_fi: a fault armed by hs_arm_fi (level R) fires in this call.
+ * abft_rel (nullable): D1 relative checksum error when the handle has
+ * detect on and project != 0, else -1. x, y: device. */
+hs_status hs_apply(hs_solver* s, const double* x, double* y, double dt_eff, int allow_fi, int project,
+                   double* abft_rel);
+/* z = r / diag (apply_preconditioner, het.cu:957-960). device. */
+hs_status hs_precond(hs_solver* s, const double* r, double* z);
+/* b = M T + dt F (build_rhs, het.cu:963-971). device. */
+hs_status hs_build_rhs(hs_solver* s, const double* T, double* b);
+/* fixed-order dot product over all nodes (HeatOperator::dot, het.cu:973-987). device. */
+hs_status hs_dot(hs_solver* s, const double* x, const double* y, double* out);
+/* Jacobi-PCG from x (pcg_solve, het.cu:994-1039), device resident; *iters
+ * as the reference returns it. b, x: device. */
+hs_status hs_pcg(hs_solver* s, const double* b, double* x, int max_iter, double tol, int* iters);
+/* arm a level-R or vector fault for the next hs_apply(allow_fi=1) / hs_pcg */
+hs_status hs_arm_fi(hs_solver* s, const hs_fi_spec* fi);
+
+/* One full trajectory from the initial condition (run_case, het.cu:1107-1259).
+ * keep_reference != 0: this run is the reference (its snapshots are kept on
+ * the device); otherwise E(t) and spread are measured against the kept
+ * reference and D3 against its per-step range.  T_final_host (nullable, Nn
+ * values) receives the final field.  out: n_steps records. */
+hs_status hs_run_case(hs_solver* s, int n_steps, int snap_every, const hs_fi_spec* fi, int reproject,
+                      int keep_reference, hs_step_record* out, double* T_final_host, int* nonfinite);
+
+/* --verify (run_verify, het.cu:1293-1338): homogeneous field required. */
+hs_status hs_verify(hs_solver* s, int n_steps, double* rel_err, long long* total_iters, double* ms);
+
+/* End-to-end solve with host buffers: copies T0 in, runs n_steps implicit-
+ * Euler steps (build_rhs + PCG), copies the field back. */
+hs_status hs_solve_host(hs_solver* s, const double* T0_host, double* T_host, int n_steps, long long* total_iters,
+                        double* device_ms);
+
+/* --diag-cg (het.cu:1491-1504): one build_rhs + PCG from the initial
+ * condition, logging the relative residual before the loop (rel0) and
+ * rel/alpha/beta per iteration (up to cap entries). */
+hs_status hs_diag_cg(hs_solver* s, int max_iter, double tol, double* rel0, double* rel, double* alpha, double* beta,
+                     int cap, int* iters);
+
+/* --dump-snaps (het.cu:1239-1245): write snap_<tag>_<case>_<step>_rank0.bin
+ * into dir at every snapshot step of later hs_run_case calls (dir null: off). */
+hs_status hs_set_dump(hs_solver* s, const char* dir, const char* tag);
+hs_status hs_set_case_tag(hs_solver* s, const char* case_tag);
+
+/* Is the fault target on the Dirichlet boundary? (target_on_boundary,
+ * het.cu:1272-1290); 1, 0, or -1 without a fault. */
+int hs_target_on_boundary(const hs_solver* s, const hs_fi_spec* fi);
+
+/* Twin-run summary and fault class (het.cu:1506-1542, 1585-1595) from the
+ * per-step records of cleanA, cleanB and the fault run (F null without a
+ * fault).  Host-only arithmetic. */
+typedef struct hs_twin_summary {
+    double E_floor_max, E_floor_final, E_fault_max, E_fault_int, E_fault_final, thr;
+    double spread_at_max, spread_final;
+    int step_at_max, iters_delta_max;
+    int d1_first, d2_first, d3_first, pad;
+    double d1_max, d2_max, d1_max_A, d2_max_A;
+    char cls[16];
+    char detected_by[16];
+} hs_twin_summary;
+hs_status hs_classify(const hs_step_record* A, const hs_step_record* B, const hs_step_record* F, int n_steps,
+                      int fi_level, int F_nonfinite, double dt, double thr_user, int detect, hs_twin_summary* out);
+
+/* The reference solver's command line (het.cu:1340-1350, 1380-1433) with its
+ * output files; returns the process exit code. */
+int hs_cli_main(int argc, char** argv);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HEAT_B200_H */

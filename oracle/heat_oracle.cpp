@@ -48,12 +48,13 @@ namespace {
 // ---- canonical reduction partition (mirrors the library's tile constants) ---
 // Interior nodes [1,N-1]^3 are cut into tiles of CX planes (x) x TY rows (y) x
 // TZ columns (z); the boundary nodes are enumerated in increasing node index
-// and cut into blocks of RT. Each tile thread (ly,lz) accumulates its column
+// and cut into blocks of RT*BPT (thread t of block b takes the nodes
+// b*RT*BPT + k*RT + t, k = 0..BPT-1, in order). Each tile thread (ly,lz) accumulates its column
 // over the tile's planes in increasing x; a block's RT values are combined by
 // a 32-lane xor butterfly per warp then an 8-way xor butterfly over warps; the
 // partials (tiles first, then boundary blocks) are combined by RT strided
 // sequential sums followed by the same block tree.
-int g_CX = 16, g_TY = 8, g_TZ = 32;
+int g_CX = 16, g_TY = 8, g_TZ = 32, g_BPT = 8;
 const int RT = 256;
 
 inline double tree256(const double* v) {
@@ -348,12 +349,18 @@ struct Oracle {
             P[t] = tree256(v);
         }
         long NB = n_boundary();
-        long nb = (NB + RT - 1) / RT;
+        const long RB = (long)RT * g_BPT;
+        long nb = (NB + RB - 1) / RB;
         for (long b = 0; b < nb; ++b) {
             double v[RT];
             for (int l = 0; l < RT; ++l) {
-                long j = b * RT + l;
-                v[l] = (j < NB) ? term(bnd_node(j), 0.0) : 0.0;
+                double acc = 0.0;
+                for (int k = 0; k < g_BPT; ++k) {
+                    long j = b * RB + (long)k * RT + l;
+                    if (j >= NB) break;
+                    acc = term(bnd_node(j), acc);
+                }
+                v[l] = acc;
             }
             P.push_back(tree256(v));
         }
@@ -445,9 +452,10 @@ struct Oracle {
         std::vector<double> ones(Nn);
         for (long n = 0; n < Nn; ++n) ones[n] = is_bnd_n(n) ? 0.0 : 1.0;
         wM.assign(Nn, 0.0); wA.assign(Nn, 0.0);
-        int save = detect; detect = 0;
+        int save = detect, save_col = colored; detect = 0; colored = 1;
         apply(ones.data(), wM.data(), 0.0, false, false, false);
         apply(ones.data(), wA.data(), dt, false, false, false);
+        colored = save_col;
         norm_wM = std::sqrt(dot(wM.data(), wM.data()));
         norm_wA = std::sqrt(dot(wA.data(), wA.data()));
         detect = save;
@@ -547,7 +555,7 @@ struct or_step_out {
     int snap;  // 1 if this step was a snapshot
 };
 
-void or_set_layout(int cx, int ty, int tz) { g_CX = cx; g_TY = ty; g_TZ = tz; }
+void or_set_layout(int cx, int ty, int tz, int bpt) { g_CX = cx; g_TY = ty; g_TZ = tz; g_BPT = bpt; }
 
 int or_set_threads(int n) {
 #ifdef _OPENMP

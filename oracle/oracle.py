@@ -61,7 +61,7 @@ def lib():
         L.or_verify.argtypes = [vp, C.c_int, C.c_int, C.c_double, C.POINTER(C.c_long)]
         L.or_get_vectors.argtypes = [vp, vp, vp, vp, vp, vp]
         L.or_get_matrices.argtypes = [vp, vp, vp, vp]
-        L.or_set_layout.argtypes = [C.c_int, C.c_int, C.c_int]
+        L.or_set_layout.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int]
         L.or_set_threads.restype = C.c_int
         L.or_set_threads.argtypes = [C.c_int]
         L.or_initial_condition.argtypes = [vp, dp]
@@ -73,9 +73,12 @@ def _ptr(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
 
 
-def set_layout(cx: int, ty: int, tz: int) -> None:
-    """Canonical reduction tile (planes, rows, columns); must match the library's."""
-    lib().or_set_layout(cx, ty, tz)
+def set_layout(cx: int, ty: int, tz: int, bpt: int = 8) -> None:
+    """Canonical reduction tile (planes, rows, columns, boundary nodes per thread).
+
+    Must equal the library's (``mnhack8_b200._lib.layout()``); the tile
+    thread count is fixed at 256."""
+    lib().or_set_layout(cx, ty, tz, bpt)
 
 
 def set_threads(n: int) -> int:

@@ -1,0 +1,114 @@
+"""C-ABI library checks that need no GPU: it loads, exports every symbol the
+header declares, its canonical layout matches the oracle, its host-side
+twin-run classifier agrees with the oracle's restatement, and the CLI keeps
+the reference's usage text, argument checks and exit codes."""
+import os
+import re
+import subprocess
+
+import pytest
+
+from mnhack8_b200 import _lib
+from tests.conftest import ROOT
+from tests.helpers import field
+
+
+def header_functions():
+    src = open(os.path.join(ROOT, "include", "heat_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(hs_[a-z_0-9]+)\s*\(", src)))
+
+
+def test_header_symbols_exported():
+    L = _lib.lib()
+    names = header_functions()
+    assert len(names) >= 20
+    for n in names:
+        assert hasattr(L, n), f"{n} declared in include/heat_b200.h but not exported"
+    assert sorted(_lib.EXPORTS) == names
+
+
+def test_api_version_and_layout(oracle):
+    assert _lib.lib().hs_api_version() == 1
+    lay = _lib.layout()
+    assert lay["rt"] == 256 and lay["ty"] * lay["tz"] == 256
+    assert (lay["cx"], lay["ty"], lay["tz"], lay["bpt"]) == (16, 8, 32, 8)
+
+
+def test_no_oracle_in_library():
+    """The product never links the oracle."""
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True, text=True).stdout
+    assert "or_create" not in out and "or_run_case" not in out
+    ldd = subprocess.run(["ldd", _lib.LIB_PATH], capture_output=True, text=True).stdout
+    assert "oracle" not in ldd
+
+
+def _cli(args):
+    return subprocess.run([_lib.CLI_PATH] + [str(a) for a in args], capture_output=True, text=True, timeout=60)
+
+
+def test_cli_usage_capabilities():
+    """The reference's validation scripts probe these flags in the usage text (vlib.capabilities)."""
+    r = _cli([])
+    assert r.returncode == 1
+    txt = r.stdout + r.stderr
+    for flag in ["--verify", "--kernel", "--scatter", "--fi-rank", "--thr", "--reproject-bc", "--detect"]:
+        assert flag in txt
+
+
+def test_cli_argument_errors(tmp_path):
+    k, r = field(4, "homogeneous")
+    pre = str(tmp_path / "h4")
+    k.tofile(pre + "_k.bin"); r.tofile(pre + "_rhoc.bin")
+    assert _cli([4, 0.01, 1e-3, pre, tmp_path, "--bogus"]).returncode == 1
+    bad = _cli([4, 0.01, 1e-3, pre, tmp_path, "--fi", 1, 0, 5, 64])
+    assert bad.returncode == 1 and "BIT must be in 0..63" in bad.stderr
+    h = _cli([4, 0.01, 1e-3, pre, tmp_path, "--fi", 3, 0, 5, 10])
+    assert h.returncode == 1 and "level H needs >= 2 ranks" in h.stderr
+    miss = _cli([4, 0.01, 1e-3, str(tmp_path / "nope"), tmp_path])
+    assert miss.returncode == 1 and "Cannot open" in miss.stderr
+    short = str(tmp_path / "short")
+    k[:10].tofile(short + "_k.bin"); r[:10].tofile(short + "_rhoc.bin")
+    s = _cli([4, 0.01, 1e-3, short, tmp_path])
+    assert s.returncode == 1 and "Field file too small" in s.stderr
+    neg = str(tmp_path / "neg")
+    kk = k.copy(); kk[3] = -1.0
+    kk.tofile(neg + "_k.bin"); r.tofile(neg + "_rhoc.bin")
+    n = _cli([4, 0.01, 1e-3, neg, tmp_path])
+    assert n.returncode == 1 and "non-positive or NaN coefficient at element 3" in n.stderr
+
+
+def test_load_fields(tmp_path):
+    import numpy as np
+    k, r = field(6, "lognormal", sigma=1.0, L=0.25, seed=2)
+    pre = str(tmp_path / "f")
+    k.tofile(pre + "_k.bin"); r.tofile(pre + "_rhoc.bin")
+    kk, rr = np.zeros(216), np.zeros(216)
+    _lib.check(_lib.lib().hs_load_fields(pre.encode(), 6, kk.ctypes.data, rr.ctypes.data))
+    assert np.array_equal(kk, k) and np.array_equal(rr, r)
+
+
+@pytest.mark.parametrize("case", ["L2_b55", "L1_b51", "L2_b62", "clean"])
+def test_classifier_matches_oracle(oracle, case):
+    """The library's twin-run summary (host C++) equals the oracle's restatement on the same records."""
+    k, r = field(12, "lognormal", sigma=1.0, L=0.25, seed=7)
+    o = oracle.Oracle(12, 5e-4, k, r, form="wht", detect=True)
+    rA = o.run_case(16, snap_every=1, keep_snaps=True)
+    rB = o.run_case(16, snap_every=1, ref_snaps=rA["snaps"])
+    if case == "clean":
+        fi, rF = None, None
+    else:
+        lv, bit = int(case[1]), int(case.split("_b")[1])
+        target = 6 * 12 * 12 + 6 * 12 + 6 if lv == 2 else 6 * 169 + 6 * 13 + 6
+        fi = (lv, 5, target, bit, 0)
+        rF = o.run_case(16, snap_every=1, fi=fi, ref_snaps=rA["snaps"])
+    lv = fi[0] if fi else 0
+    want = oracle.classify(rA, rB, rF, lv, 5e-4, detect=True)
+    got = _lib.classify(rA["steps"], rB["steps"], rF["steps"] if rF else None, lv, 5e-4, detect=True,
+                        F_nonfinite=rF["nonfinite"] if rF else 0)
+    assert got["cls"] == want["cls"]
+    assert got["detected_by"] == want["detected_by"]
+    for key in ("E_floor_max", "E_fault_max", "E_fault_int", "E_fault_final", "thr", "spread_at_max",
+                "spread_final", "step_at_max", "iters_delta_max", "d1_first", "d2_first", "d3_first", "d1_max",
+                "d2_max"):
+        assert got[key] == want[key] or (got[key] != got[key] and want[key] != want[key]), key
