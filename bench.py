@@ -1,0 +1,353 @@
+#!/usr/bin/env python3
+"""Throughput of the transient-heat PCG hot path on B200 (one JSON line).
+
+Workload (one "step" of this benchmark): one complete implicit-Euler
+trajectory of the FP64 N=128 problem -- 128^3 Q1 elements (129^3 = 2,146,689
+nodes) on the unit cube, lognormal conductivity ln k ~ N(0, 1) with Gaussian
+correlation length 8 elements (seeded synthetic field, the reference
+generator's FFT algorithm), rho*c = 1, Dirichlet T = 0, Gaussian initial bump
+(sigma 0.15), source off, dt = 1e-4, 50 steps, each a Jacobi-PCG solve to
+relative residual 1e-10 with the ABFT checksum (D1) on every operator apply,
+deterministic (colored) scatter.  Metric: DOF-iterations per second =
+(N+1)^3 x total CG iterations / time (the reference's solve_ms definition:
+build_rhs + PCG).
+
+value: device time (CUDA events) of K trajectories with every input resident
+in HBM.  e2e: the same through the public C ABI with host buffers
+(hs_solve_host: pinned initial field in, 50 steps, final field out).  The
+working set (~170 MB of node and element arrays) exceeds the 126 MB L2.
+
+--impl reference: the reference path on the host cores: the CPU restatement
+of the reference solver (its dense `fast` element form, colored order), run
+on a bounded sample of the same workload each step.
+
+Multi-GPU (torchrun): replicas only -- every rank solves its own seeded
+instance, no collective on the data path; value = all ranks' DOF-iterations
+/ the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_DEFAULT = 128
+DT = 1e-4
+STEPS_PER_TRAJ = 50
+RTOL = 1e-10
+IC_SIGMA = 0.15
+CORR_ELEMENTS = 8.0
+METRIC = "DOF-iters/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10, help="timed trajectories")
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--N", type=int, default=N_DEFAULT)
+    ap.add_argument("--kernel", default="wht", choices=["wht", "fast", "gauss"])
+    ap.add_argument("--scatter", default="colored", choices=["colored", "atomic"])
+    ap.add_argument("--no-detect", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="only the timed trajectories (no e2e, kernel timing or CPU baseline): for ncu captures")
+    return ap.parse_args()
+
+
+def make_field(N, seed):
+    from mnhack8_b200.fields import FieldSpec, make_field as mk
+    k, r, _ = mk(FieldSpec(n=N, model="lognormal", mu=0.0, sigma=1.0, L=CORR_ELEMENTS / N, seed=seed))
+    return k.ravel(), r.ravel()
+
+
+def workload_config(args, world):
+    return {
+        "workload": f"implicit-Euler trajectory, Q1 hex N={args.N}^3 elements ({(args.N + 1) ** 3} nodes), "
+                    f"lognormal k sigma=1 corr=8 elements, Gaussian IC sigma=0.15, dt=1e-4, {STEPS_PER_TRAJ} steps, "
+                    f"Jacobi-PCG rtol 1e-10, ABFT D1 {'off' if args.no_detect else 'on'}, {args.scatter} scatter",
+        "N": args.N, "nodes": (args.N + 1) ** 3, "elements": args.N ** 3, "time_steps_per_step": STEPS_PER_TRAJ,
+        "dt": DT, "rtol": RTOL, "element_form": args.kernel, "scatter": args.scatter,
+        "abft": not args.no_detect, "precision": "fp64",
+        "l2": "inputs larger than L2 (~170 MB working set vs 126 MB L2)",
+        "parallelism": f"replicas x{world}",
+    }
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(N):
+    """dram bytes per launch of the PCG operator kernel from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", f"k_apply_colored_loop_N{N}.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "100", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, ValueError):
+            self.proc = None
+        time.sleep(0.25)
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.15)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline_sample(N, seconds, threads=None, form="fast"):
+    """Time the CPU restatement of the reference solver on a bounded sample of the
+    workload: build_rhs + CG iterations of one implicit-Euler step of the same
+    problem, iterations capped so the sample takes about `seconds`."""
+    from oracle import oracle as om
+    n = om.set_threads(threads or os.cpu_count() or 1)
+    k, r = make_field(N, 1)
+    o = om.Oracle(N, DT, k, r, form=form, colored=True, detect=True, no_source=True, ic="gaussian",
+                  ic_sigma=IC_SIGMA)
+    T = o.initial_condition()
+    t0 = time.perf_counter()
+    b = o.build_rhs(T)
+    it1, _, _ = o.pcg(b, T, 1, RTOL)
+    per_iter = max(time.perf_counter() - t0, 1e-3)
+    cap = int(max(1, min(200, seconds / per_iter)))
+    t0 = time.perf_counter()
+    b = o.build_rhs(T)
+    it, _, _ = o.pcg(b, T, cap, RTOL)
+    dt = time.perf_counter() - t0
+    nodes = (N + 1) ** 3
+    return {"value": nodes * it / dt, "unit": METRIC, "cores": n, "kind": "port",
+            "sample": f"one implicit-Euler step of the same N={N} problem (build_rhs + {it} CG iterations of the "
+                      f"dense reference element form, colored order, ABFT on), {dt:.1f} s on {n} host threads"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import oracle as om
+    n_threads = om.set_threads(os.cpu_count() or 1)
+    k, r = make_field(args.N, 1)
+    o = om.Oracle(args.N, DT, k, r, form="fast", colored=args.scatter == "colored", detect=not args.no_detect,
+                  no_source=True, ic="gaussian", ic_sigma=IC_SIGMA)
+    T = o.initial_condition()
+    cap = 3      # CG iterations per bounded sample step
+    for _ in range(args.warmup):
+        o.pcg(o.build_rhs(T), T, cap, RTOL)
+    tot_it, t0 = 0, time.perf_counter()
+    for _ in range(args.steps):
+        it, _, _ = o.pcg(o.build_rhs(T), T, cap, RTOL)
+        tot_it += it
+    dt = time.perf_counter() - t0
+    nodes = (args.N + 1) ** 3
+    v = nodes * tot_it / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded lognormal field)",
+        "config": dict(workload_config(args, 1), element_form="fast (reference dense 8x8)"),
+        "cpu_baseline": {"value": v, "unit": METRIC, "cores": n_threads, "kind": "port",
+                         "sample": f"each step: build_rhs + {cap} CG iterations of one implicit-Euler step of the "
+                                   f"same problem (CPU restatement of the reference solver, dense element form)"},
+        "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    from mnhack8_b200 import _lib
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(local)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier(device_ids=[local])
+        torch.cuda.synchronize()
+
+    N = args.N
+    nodes, elems = (N + 1) ** 3, N ** 3
+    k, r = make_field(N, 1 + rank)
+    g = _lib.Solver(N, DT, k, r, kernel=args.kernel, scatter=args.scatter, detect=not args.no_detect,
+                    no_source=True, ic="gaussian", ic_sigma=IC_SIGMA, rtol=RTOL, max_iter=500, device=local)
+    # warm-up trajectories (graph instantiation, clocks)
+    for _ in range(args.warmup):
+        g.advance(STEPS_PER_TRAJ, from_ic=True)
+    barrier()
+    sampler = ClockSampler(local)
+    with sampler:
+        barrier()
+        tot_it, tot_ms = 0, 0.0
+        for _ in range(args.steps):
+            it, ms = g.advance(STEPS_PER_TRAJ, from_ic=True)
+            tot_it += it
+            tot_ms += ms
+        barrier()
+    clocks = sampler.summary()
+    # slowest rank's device time, all ranks' work
+    t = torch.tensor([tot_ms, float(tot_it)], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        tmax = t.clone()
+        dist.all_reduce(tmax[0:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(tmax[1:2], op=dist.ReduceOp.SUM)
+        t = tmax
+    ms_total, it_all = float(t[0]), float(t[1])
+    value = nodes * it_all / (ms_total * 1e-3)
+    if args.profile:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "profile_run": True}), flush=True)
+        g.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
+
+    # ---- end to end through the C ABI with pinned host buffers -------------------
+    T0 = torch.empty(nodes, dtype=torch.float64, pin_memory=True)
+    T0.copy_(torch.from_numpy(_initial(g, N)))
+    Tout = torch.empty(nodes, dtype=torch.float64, pin_memory=True)
+    g.solve_host_ptr(T0.data_ptr(), Tout.data_ptr(), STEPS_PER_TRAJ)   # warm
+    barrier()
+    e2e_it, t0 = 0, time.perf_counter()
+    for _ in range(args.steps):
+        it, _ = g.solve_host_ptr(T0.data_ptr(), Tout.data_ptr(), STEPS_PER_TRAJ)
+        e2e_it += it
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s, float(e2e_it)], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(te[0:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(te[1:2], op=dist.ReduceOp.SUM)
+    e2e_value = nodes * float(te[1]) / float(te[0])
+
+    # ---- roofline of the dominant kernel (the fused PCG operator kernel) ----------
+    ms_k1 = g.time_kernel(0, reps=20)
+    ms_k2 = g.time_kernel(1, reps=20)
+    detect = not args.no_detect
+    alg_k1 = (40 if detect else 32) * nodes + 16 * elems   # read z, p_old[, w]; write p, Ap; read k, rho*c
+    alg_k2 = 64 * nodes                                     # read x, p, Ap, r, d; write x, r, z
+    peak, peak_kind = peaks()
+    ach = alg_k1 / (ms_k1 * 1e-3) / 1e9
+    traffic = profile_traffic(N)
+    iters_per_traj = it_all / max(1, world) / args.steps
+    launches = int(round(args.steps * (STEPS_PER_TRAJ * 5 + 2 * iters_per_traj)))
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded lognormal conductivity, FFT Gaussian-field algorithm of the reference generator)",
+        "config": workload_config(args, world),
+        "cg_iters_per_trajectory": iters_per_traj,
+        "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                     "traffic": traffic, "kernel": "k_apply_colored (PCG operator: p = z + beta p, Ap = A p, "
+                     "p.Ap and ABFT partials)", "alg_bytes_per_launch": alg_k1, "ms_per_launch": ms_k1,
+                     "peak_source": f"{peak_kind} hbm_gbs", "l2": "flushed before each timed launch",
+                     "update_kernel": {"ms_per_launch": ms_k2, "alg_bytes_per_launch": alg_k2,
+                                       "achieved": alg_k2 / (ms_k2 * 1e-3) / 1e9}},
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": nodes * 8, "d2h_bytes_per_step": nodes * 8},
+        "gpu_launches": launches,
+        "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"]},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_sample(N, args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    g.close()
+    if dist is not None:
+        dist.barrier(device_ids=[local])
+        dist.destroy_process_group()
+    return 0
+
+
+def _initial(g, N):
+    from mnhack8_b200 import _lib  # noqa: F401
+    g.advance(0, from_ic=True)           # puts the initial condition into the solver's field
+    return g.get_field()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

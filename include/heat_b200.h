@@ -149,6 +149,21 @@ hs_status hs_verify(hs_solver* s, int n_steps, double* rel_err, long long* total
 hs_status hs_solve_host(hs_solver* s, const double* T0_host, double* T_host, int n_steps, long long* total_iters,
                         double* device_ms);
 
+/* Advance the device-resident field n_steps implicit-Euler steps (build_rhs +
+ * PCG each, no host traffic); from_ic != 0 restarts from the initial
+ * condition (kept on the device) first.  Device time and CG iterations.
+ * hs_set_field / hs_get_field move the field (host buffers). */
+hs_status hs_advance(hs_solver* s, int n_steps, int from_ic, long long* total_iters, double* device_ms);
+hs_status hs_set_field(hs_solver* s, const double* T_host);
+hs_status hs_get_field(hs_solver* s, double* T_host);
+
+/* Per-launch device time of one kernel of the hot path, averaged over reps
+ * launches with the L2 cache flushed before each (which: 0 the PCG operator
+ * kernel p = z + beta p, Ap = A p with its p.Ap and checksum partials; 1 the
+ * PCG vector update; 2 a plain projected apply y = A x).  Leaves the solver
+ * state to be re-initialised by the next run. */
+hs_status hs_time_kernel(hs_solver* s, int which, int reps, double* ms_per_launch);
+
 /* --diag-cg (het.cu:1491-1504): one build_rhs + PCG from the initial
  * condition, logging the relative residual before the loop (rel0) and
  * rel/alpha/beta per iteration (up to cap entries). */

@@ -24,7 +24,8 @@ EXPORTS = [
     "hs_default_options", "hs_last_error", "hs_api_version", "hs_get_layout", "hs_load_fields", "hs_create",
     "hs_destroy", "hs_num_nodes", "hs_field_stats", "hs_apply", "hs_precond", "hs_build_rhs", "hs_dot", "hs_pcg",
     "hs_arm_fi", "hs_run_case", "hs_verify", "hs_solve_host", "hs_diag_cg", "hs_set_dump", "hs_set_case_tag",
-    "hs_target_on_boundary", "hs_classify", "hs_cli_main",
+    "hs_target_on_boundary", "hs_classify", "hs_cli_main", "hs_advance", "hs_set_field", "hs_get_field",
+    "hs_time_kernel",
 ]
 
 
@@ -120,6 +121,14 @@ def lib():
     L.hs_classify.restype = i
     L.hs_classify.argtypes = [C.POINTER(StepRecord), C.POINTER(StepRecord), C.POINTER(StepRecord), i, i, i, d, d,
                               i, C.POINTER(TwinSummary)]
+    L.hs_advance.restype = i
+    L.hs_advance.argtypes = [vp, i, i, C.POINTER(ll), pd]
+    L.hs_set_field.restype = i
+    L.hs_set_field.argtypes = [vp, vp]
+    L.hs_get_field.restype = i
+    L.hs_get_field.argtypes = [vp, vp]
+    L.hs_time_kernel.restype = i
+    L.hs_time_kernel.argtypes = [vp, i, i, pd]
     L.hs_cli_main.restype = i
     L.hs_cli_main.argtypes = [i, C.POINTER(C.c_char_p)]
     _lib = L
@@ -249,6 +258,34 @@ class Solver:
         tot, ms = C.c_longlong(), C.c_double()
         check(lib().hs_solve_host(self._h, T0.ctypes.data, T.ctypes.data, int(n_steps), C.byref(tot), C.byref(ms)))
         return T, tot.value, ms.value
+
+    def set_field(self, T):
+        T = _host(T)
+        check(lib().hs_set_field(self._h, T.ctypes.data))
+
+    def get_field(self):
+        T = np.empty(self.Nn)
+        check(lib().hs_get_field(self._h, T.ctypes.data))
+        return T
+
+    def advance(self, n_steps, from_ic=False):
+        """n_steps device-resident steps (optionally restarting from the initial
+        condition kept on the device); returns (total CG iterations, device ms)."""
+        tot, ms = C.c_longlong(), C.c_double()
+        check(lib().hs_advance(self._h, int(n_steps), int(from_ic), C.byref(tot), C.byref(ms)))
+        return tot.value, ms.value
+
+    def solve_host_ptr(self, T0_ptr, T_ptr, n_steps):
+        """hs_solve_host on caller-owned (e.g. pinned) host buffers given as addresses."""
+        tot, ms = C.c_longlong(), C.c_double()
+        check(lib().hs_solve_host(self._h, T0_ptr, T_ptr, int(n_steps), C.byref(tot), C.byref(ms)))
+        return tot.value, ms.value
+
+    def time_kernel(self, which, reps=20):
+        """Average per-launch device ms of one hot-path kernel (L2 flushed before each launch)."""
+        ms = C.c_double()
+        check(lib().hs_time_kernel(self._h, int(which), int(reps), C.byref(ms)))
+        return ms.value
 
     def diag_cg(self, max_iter=500, tol=1e-8):
         cap = max_iter + 1

@@ -73,6 +73,7 @@ struct hs_solver {
     DevBuf<double> red;                 // standalone reduction outputs
     DevBuf<unsigned long long> sp;      // spread: [gmax bits, count]
     DevBuf<double> logs;                // diag-cg log buffers (3 * cap)
+    DevBuf<double> T0;                  // initial condition kept on the device (hs_advance)
     bool has_F = false;
 
     // PCG graphs built on first use: [0] step (RHS + PCG), [1] PCG only
@@ -829,6 +830,112 @@ hs_status hs_diag_cg(hs_solver* h, int max_iter, double tol, double* rel0, doubl
     hsx.log_rel = hsx.log_alpha = hsx.log_beta = nullptr; hsx.log_cap = 0;
     HS_CUDA(cudaMemcpy(h->st.p, &hsx, sizeof(hsx), cudaMemcpyHostToDevice));
     return sync_state_config(h, h->opt.max_iter, h->opt.rtol);
+}
+
+}  // extern "C"
+
+extern "C" {
+
+hs_status hs_set_field(hs_solver* h, const double* T_host) {
+    if (!h || !T_host) return HS_ERR_ARG;
+    HS_CUDA(cudaMemcpyAsync(h->T.p, T_host, h->Nn * 8, cudaMemcpyHostToDevice, h->s));
+    HS_CUDA(cudaStreamSynchronize(h->s));
+    return HS_OK;
+}
+
+hs_status hs_get_field(hs_solver* h, double* T_host) {
+    if (!h || !T_host) return HS_ERR_ARG;
+    HS_CUDA(cudaMemcpyAsync(T_host, h->T.p, h->Nn * 8, cudaMemcpyDeviceToHost, h->s));
+    HS_CUDA(cudaStreamSynchronize(h->s));
+    return HS_OK;
+}
+
+hs_status hs_advance(hs_solver* h, int n_steps, int from_ic, long long* total_iters, double* device_ms) {
+    if (!h || n_steps < 0) return HS_ERR_ARG;
+    hs_status st = build_graph(h, 0);
+    if (st != HS_OK) return st;
+    if (from_ic && !h->T0.p) {
+        std::vector<double> v(h->Nn, 0.0);
+        if (h->opt.ic_mode == 1) gaussian_ic(h->N, h->opt.ic_sigma, v.data());
+        HS_CUDA(h->T0.alloc(h->Nn));
+        HS_CUDA(cudaMemcpy(h->T0.p, v.data(), h->Nn * 8, cudaMemcpyHostToDevice));
+    }
+    DevBuf<int> d_it;
+    DevBuf<double> d_d1;
+    HS_CUDA(d_it.alloc(std::max(n_steps, 1)));
+    HS_CUDA(d_d1.alloc(std::max(n_steps, 1)));
+    cudaEvent_t e0, e1;
+    HS_CUDA(cudaEventCreate(&e0)); HS_CUDA(cudaEventCreate(&e1));
+    HS_CUDA(cudaEventRecord(e0, h->s));
+    if (from_ic) HS_CUDA(cudaMemcpyAsync(h->T.p, h->T0.p, h->Nn * 8, cudaMemcpyDeviceToDevice, h->s));
+    for (int step = 0; step < n_steps; ++step) {
+        st = enqueue_step(h, nullptr, step, 0, d_it.p + step, d_d1.p + step, nullptr, nullptr);
+        if (st != HS_OK) return st;
+    }
+    HS_CUDA(cudaEventRecord(e1, h->s));
+    HS_CUDA(cudaEventSynchronize(e1));
+    float fms = 0.f;
+    HS_CUDA(cudaEventElapsedTime(&fms, e0, e1));
+    cudaEventDestroy(e0); cudaEventDestroy(e1);
+    std::vector<int> it(std::max(n_steps, 1));
+    HS_CUDA(cudaMemcpy(it.data(), d_it.p, n_steps * sizeof(int), cudaMemcpyDeviceToHost));
+    long long tot = 0;
+    for (int i = 0; i < n_steps; ++i) tot += it[i];
+    if (total_iters) *total_iters = tot;
+    if (device_ms) *device_ms = fms;
+    return HS_OK;
+}
+
+hs_status hs_time_kernel(hs_solver* h, int which, int reps, double* ms_per_launch) {
+    if (!h || reps < 1 || which < 0 || which > 2) return HS_ERR_ARG;
+    // state for repeated launches: loop running at iteration 1, never converging
+    DevState hsx{};
+    HS_CUDA(cudaMemcpy(&hsx, h->st.p, sizeof(hsx), cudaMemcpyDeviceToHost));
+    DevState saved = hsx;
+    hsx.done = 0; hsx.broken = 0; hsx.iter = 1; hsx.beta = 0.5; hsx.rho = 1.0; hsx.alpha = 1e-3;
+    hsx.bnorm = 1.0; hsx.tol = 0.0; hsx.max_iter = 1 << 30; hsx.fi_armR = 0; hsx.fi_vec = 0;
+    hsx.log_rel = hsx.log_alpha = hsx.log_beta = nullptr; hsx.log_cap = 0;
+    HS_CUDA(cudaMemcpy(h->st.p, &hsx, sizeof(hsx), cudaMemcpyHostToDevice));
+    // nonzero, SPD-consistent inputs (p.Ap > 0): the positive diagonal
+    for (double* v : {h->z.p, h->p0.p, h->p1.p, h->T.p, h->r.p})
+        k_copy<<<grid_for(h->Nn, RT), RT, 0, h->s>>>(h->Nn, h->diag.p, v);
+    // L2 flush buffer (256 MiB > 126 MB L2)
+    DevBuf<char> flush;
+    const size_t fl = (size_t)256 << 20;
+    HS_CUDA(flush.alloc(fl));
+    std::vector<cudaEvent_t> ev(2 * (size_t)reps);
+    for (auto& e : ev) HS_CUDA(cudaEventCreate(&e));
+    const bool det = h->opt.detect != 0;
+    for (int r = 0; r < reps; ++r) {
+        HS_CUDA(cudaMemsetAsync(flush.p, r & 0xff, fl, h->s));
+        HS_CUDA(cudaEventRecord(ev[2 * r], h->s));
+        if (which == 0) {
+            apply_projected(h, ROLE_LOOP, nullptr, h->Ap.p, h->opt.dt, det, h->wA.p, nullptr, 0.0);
+        } else if (which == 1) {
+            // keep the iteration counter (and so the p buffer) fixed at 1
+            launch_update(h, UPD_LOOP, false);
+        } else {
+            apply_projected(h, ROLE_PLAIN, h->T.p, h->z.p, h->opt.dt, false, nullptr, nullptr, 0.0);
+        }
+        HS_CUDA(cudaEventRecord(ev[2 * r + 1], h->s));
+        if (which == 1) {
+            DevState* d = h->st.p;
+            HS_CUDA(cudaMemcpyAsync(&d->iter, &hsx.iter, sizeof(int), cudaMemcpyHostToDevice, h->s));
+        }
+    }
+    HS_CUDA(cudaStreamSynchronize(h->s));
+    HS_CUDA(cudaGetLastError());
+    double tot = 0;
+    for (int r = 0; r < reps; ++r) {
+        float ms = 0.f;
+        HS_CUDA(cudaEventElapsedTime(&ms, ev[2 * r], ev[2 * r + 1]));
+        tot += ms;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    saved.done = 1;
+    HS_CUDA(cudaMemcpy(h->st.p, &saved, sizeof(saved), cudaMemcpyHostToDevice));
+    if (ms_per_launch) *ms_per_launch = tot / reps;
+    return HS_OK;
 }
 
 }  // extern "C"
