@@ -314,7 +314,12 @@ def main():
     ach = alg_k1 / (ms_k1 * 1e-3) / 1e9
     traffic = profile_traffic(N)
     iters_per_traj = it_all / max(1, world) / args.steps
-    launches = int(round(args.steps * (STEPS_PER_TRAJ * 5 + 2 * iters_per_traj)))
+    # per time step: step begin/end, RHS and x0 operator (+ final each with ABFT),
+    # PCG prologue (update + final); per CG iteration: operator tiles + boundary
+    # + final, update + final
+    per_step = (2 + 2 * (3 if detect else 2) + 2) if args.scatter == "colored" else 12
+    per_iter = 5 if args.scatter == "colored" else 6
+    launches = int(round(args.steps * (STEPS_PER_TRAJ * per_step + per_iter * iters_per_traj)))
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,

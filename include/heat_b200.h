@@ -93,13 +93,15 @@ typedef struct hs_step_record {
     double solve_ms;    /* build_rhs + PCG (+ reprojection) device time of the step */
 } hs_step_record;
 
-/* canonical reduction tile: planes (x), rows (y), columns (z), threads */
-typedef struct hs_layout_info { int cx, ty, tz, rt, bpt; } hs_layout_info;
+/* canonical reduction orders of an N-element grid: the operator's tile
+ * (planes cx, rows ty, columns tz; rt threads; bpt boundary nodes per thread)
+ * and the flat order's nodes per thread kf */
+typedef struct hs_layout_info { int cx, ty, tz, rt, bpt, kf; } hs_layout_info;
 
 void        hs_default_options(hs_options* opt);
 const char* hs_last_error(void);               /* message of the last failing call on this thread */
 int         hs_api_version(void);
-void        hs_get_layout(hs_layout_info* out);
+void        hs_get_layout(int N, hs_layout_info* out);
 
 /* Read <prefix>_k.bin and <prefix>_rhoc.bin (N^3 float64 each) into host
  * buffers; rejects short files and non-positive/NaN values

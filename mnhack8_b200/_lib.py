@@ -47,7 +47,8 @@ class StepRecord(C.Structure):
 
 
 class LayoutInfo(C.Structure):
-    _fields_ = [("cx", C.c_int), ("ty", C.c_int), ("tz", C.c_int), ("rt", C.c_int), ("bpt", C.c_int)]
+    _fields_ = [("cx", C.c_int), ("ty", C.c_int), ("tz", C.c_int), ("rt", C.c_int), ("bpt", C.c_int),
+                ("kf", C.c_int)]
 
 
 class TwinSummary(C.Structure):
@@ -82,7 +83,7 @@ def lib():
     L.hs_default_options.argtypes = [C.POINTER(Options)]
     L.hs_last_error.restype = C.c_char_p
     L.hs_api_version.restype = i
-    L.hs_get_layout.argtypes = [C.POINTER(LayoutInfo)]
+    L.hs_get_layout.argtypes = [i, C.POINTER(LayoutInfo)]
     L.hs_load_fields.restype = i
     L.hs_load_fields.argtypes = [C.c_char_p, i, vp, vp]
     L.hs_create.restype = i
@@ -140,10 +141,11 @@ def check(status):
         raise HeatError(status, lib().hs_last_error().decode(errors="replace"))
 
 
-def layout():
+def layout(N=128):
+    """Canonical reduction orders the library uses for an N-element grid."""
     li = LayoutInfo()
-    lib().hs_get_layout(C.byref(li))
-    return dict(cx=li.cx, ty=li.ty, tz=li.tz, rt=li.rt, bpt=li.bpt)
+    lib().hs_get_layout(int(N), C.byref(li))
+    return dict(cx=li.cx, ty=li.ty, tz=li.tz, rt=li.rt, bpt=li.bpt, kf=li.kf)
 
 
 def _host(a):

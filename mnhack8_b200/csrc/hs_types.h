@@ -4,23 +4,45 @@
 
 namespace hs {
 
-// ---- canonical tile / reduction partition ----------------------------------
-// Interior nodes [1, N-1]^3 are covered by tiles of TY rows x TZ columns that
-// stream CX planes in x; one CTA of RT threads per tile, one node column per
-// thread.  Boundary nodes (any coordinate 0 or N), enumerated in increasing
-// node index, are covered by blocks of RT*BPT nodes, thread t taking nodes
-// b*RT*BPT + k*RT + t for k = 0..BPT-1.  Every reduction over node vectors in
-// the library follows this partition: a thread accumulates its nodes in
-// order, a CTA combines its RT values by a 32-lane xor butterfly per warp and
-// an 8-way xor butterfly over the warp sums, and the last CTA to finish
-// combines the per-CTA partials (tiles first, then boundary blocks) by RT
-// strided sequential sums and the same CTA tree.  The result is therefore a
-// fixed function of the inputs, independent of scheduling.
+// ---- canonical partitions and reduction orders ------------------------------
+// APPLY partition (operator kernels): interior nodes [1, N-1]^3 are covered by
+// tiles of TY rows x TZ columns streaming cx(N) planes in x, one node column
+// per reduction thread; boundary nodes (any coordinate 0 or N), enumerated in
+// increasing node index, by blocks of RT*BPT nodes, thread t taking nodes
+// b*RT*BPT + k*RT + t for k = 0..BPT-1.  The p.Ap and ABFT partials follow it.
+// FLAT partition (every other reduction and the PCG vector update): blocks of
+// RT*KF consecutive nodes, thread t of block b taking the KF consecutive nodes
+// b*RT*KF + t*KF + k.
+// In both, a thread accumulates its nodes in order, a block combines its RT
+// values by a 32-lane xor butterfly per warp and an 8-way xor butterfly over
+// the warp sums, and the last block to finish combines the per-block partials
+// (apply: tiles first, then boundary blocks) by RT strided sequential sums and
+// the same block tree.  Every result is a fixed function of the inputs,
+// independent of scheduling.
 constexpr int TY = 8;
 constexpr int TZ = 32;
-constexpr int CX = 16;
 constexpr int RT = 256;
 constexpr int BPT = 8;
+constexpr int KF = 2;
+constexpr int APPLY_SLOTS = 592;   // co-resident operator tiles assumed by cx(N): 148 SMs x 4
+
+// planes per apply tile: the cx in [8, 64] minimising (waves x (cx + 1) element
+// planes) for APPLY_SLOTS co-resident tiles
+inline int apply_cx(int N) {
+    const long long I = N - 1;
+    if (I <= 0) return 16;
+    const long long col = ((I + TY - 1) / TY) * ((I + TZ - 1) / TZ);
+    int best = 16;
+    long long best_cost = -1;
+    for (int cx = 8; cx <= 64; ++cx) {
+        const long long chunks = (I + cx - 1) / cx;
+        const long long blocks = col * chunks;
+        const long long waves = (blocks + APPLY_SLOTS - 1) / APPLY_SLOTS;
+        const long long cost = waves * ((cx < I ? cx : I) + 1);
+        if (best_cost < 0 || cost < best_cost) { best_cost = cost; best = cx; }
+    }
+    return best;
+}
 constexpr int EY = TY + 1;            // element rows touched by a tile
 constexpr int EZ = TZ + 1;            // element columns touched by a tile
 constexpr int LY = TY + 2;            // node rows loaded per plane (with halo)

@@ -45,7 +45,13 @@
 
 namespace {
 
-// ---- canonical reduction partition (mirrors the library's tile constants) ---
+// ---- canonical reduction partitions (mirror the library's) --------------------
+// Two fixed orders.  The APPLY order (the operator kernel's p.Ap and ABFT
+// partials) follows the operator's tiles, described below.  The FLAT order
+// (every other reduction: the PCG vector dots, D2, E(t), plain dots) cuts the
+// node index range into blocks of RT*KF consecutive nodes, thread t of block
+// b accumulating the KF consecutive nodes b*RT*KF + t*KF + k, k = 0..KF-1, in
+// order; blocks are combined like the apply order's partials.
 // Interior nodes [1,N-1]^3 are cut into tiles of CX planes (x) x TY rows (y) x
 // TZ columns (z); the boundary nodes are enumerated in increasing node index
 // and cut into blocks of RT*BPT (thread t of block b takes the nodes
@@ -54,8 +60,28 @@ namespace {
 // a 32-lane xor butterfly per warp then an 8-way xor butterfly over warps; the
 // partials (tiles first, then boundary blocks) are combined by RT strided
 // sequential sums followed by the same block tree.
-int g_CX = 16, g_TY = 8, g_TZ = 32, g_BPT = 8;
+int g_TY = 8, g_TZ = 32, g_BPT = 8;   // apply layout (tiles + boundary blocks); cx = apply_cx(N)
+int g_KF = 2;                                       // flat layout: consecutive nodes per thread
 const int RT = 256;
+
+// planes per apply tile as a function of N (the library's choice: the cx in
+// [8, 64] minimising waves x (cx + 1) for 592 co-resident operator tiles)
+int apply_cx(int N) {
+    const long I = N - 1;
+    if (I <= 0) return 16;
+    const long col = ((I + 8 - 1) / 8) * ((I + 32 - 1) / 32);
+    int best = 16;
+    long best_cost = -1;
+    for (int cx = 8; cx <= 64; ++cx) {
+        const long chunks = (I + cx - 1) / cx;
+        const long blocks = col * chunks;
+        const long waves = (blocks + 592 - 1) / 592;
+        const long cost = waves * ((cx < I ? cx : I) + 1);
+        if (best_cost < 0 || cost < best_cost) { best_cost = cost; best = cx; }
+    }
+    return best;
+}
+int g_cx_override = 0;   // or_set_layout: fixed cx instead of apply_cx(N)
 
 inline double tree256(const double* v) {
     double ws[8];
@@ -329,7 +355,8 @@ struct Oracle {
     double creduce(Term term) const {
         std::vector<double> P;
         const int I = N - 1;
-        const int NTX = (I + g_CX - 1) / g_CX, NTY = (I + g_TY - 1) / g_TY, NTZ = (I + g_TZ - 1) / g_TZ;
+        const int CXN = g_cx_override ? g_cx_override : apply_cx(N);
+        const int NTX = (I + CXN - 1) / CXN, NTY = (I + g_TY - 1) / g_TY, NTZ = (I + g_TZ - 1) / g_TZ;
         const int nt = (I > 0) ? NTX * NTY * NTZ : 0;
         P.resize(nt);
         #pragma omp parallel for schedule(static)
@@ -341,7 +368,7 @@ struct Oracle {
                 double acc = 0.0;
                 int iy = 1 + ty * g_TY + ly, iz = 1 + tz * g_TZ + lz;
                 if (ly < g_TY && iy <= I && iz <= I) {
-                    int x0 = 1 + tx * g_CX, x1 = std::min(tx * g_CX + g_CX, I);
+                    int x0 = 1 + tx * CXN, x1 = std::min(tx * CXN + CXN, I);
                     for (int ix = x0; ix <= x1; ++ix) acc = term(nid(ix, iy, iz), acc);
                 }
                 v[l] = acc;
@@ -372,7 +399,37 @@ struct Oracle {
         }
         return tree256(v);
     }
+    template <class Term>
+    double freduce(Term term) const {
+        const long RB = (long)RT * g_KF;
+        const long nb = (Nn + RB - 1) / RB;
+        std::vector<double> P(nb);
+        #pragma omp parallel for schedule(static)
+        for (long b = 0; b < nb; ++b) {
+            double v[RT];
+            for (int l = 0; l < RT; ++l) {
+                double acc = 0.0;
+                for (int k = 0; k < g_KF; ++k) {
+                    const long n = b * RB + (long)l * g_KF + k;
+                    if (n >= Nn) break;
+                    acc = term(n, acc);
+                }
+                v[l] = acc;
+            }
+            P[b] = tree256(v);
+        }
+        double v[RT];
+        for (int l = 0; l < RT; ++l) {
+            double acc = 0.0;
+            for (size_t q = l; q < P.size(); q += RT) acc = acc + P[q];
+            v[l] = acc;
+        }
+        return tree256(v);
+    }
     double dot(const double* a, const double* b) const {
+        return freduce([&](long n, double acc) { return std::fma(a[n], b[n], acc); });
+    }
+    double adot(const double* a, const double* b) const {   // apply order
         return creduce([&](long n, double acc) { return std::fma(a[n], b[n], acc); });
     }
     double one_int(long n) const { return is_bnd_n(n) ? 0.0 : 1.0; }
@@ -391,8 +448,8 @@ struct Oracle {
             const double* w = (dt_eff == 0.0) ? wM.data() : wA.data();
             const double nw = (dt_eff == 0.0) ? norm_wM : norm_wA;
             double s = creduce([&](long n, double acc) { return std::fma(one_int(n), y[n], acc); });
-            double c = dot(w, x);
-            double nx = std::sqrt(dot(x, x));
+            double c = adot(w, x);
+            double nx = std::sqrt(adot(x, x));
             rel = std::fabs(s - c) / std::fma(nw, nx, 1e-300);
             if (!std::isfinite(rel)) rel = 1e300;
             abft_step_max = std::fmax(abft_step_max, rel);
@@ -492,14 +549,14 @@ struct Oracle {
             if (vec_level == LV_AP && it == vec_iter) Ap[vec_idx] = flip(Ap[vec_idx], fi_bit);
             if (detect) {
                 double s = creduce([&](long n, double acc) { return std::fma(one_int(n), Ap[n], acc); });
-                double c = dot(wA.data(), p);
-                double nx = std::sqrt(dot(p, p));
+                double c = adot(wA.data(), p);
+                double nx = std::sqrt(adot(p, p));
                 double rel = std::fabs(s - c) / std::fma(norm_wA, nx, 1e-300);
                 if (!std::isfinite(rel)) rel = 1e300;
                 abft_step_max = std::fmax(abft_step_max, rel);
                 abft_calls++;
             }
-            double pAp = dot(p, Ap);
+            double pAp = adot(p, Ap);
             if (std::fabs(pAp) < 1e-30) break;
             double alpha = rho / pAp;
             for (long n = 0; n < Nn; ++n) {
@@ -555,7 +612,10 @@ struct or_step_out {
     int snap;  // 1 if this step was a snapshot
 };
 
-void or_set_layout(int cx, int ty, int tz, int bpt) { g_CX = cx; g_TY = ty; g_TZ = tz; g_BPT = bpt; }
+void or_set_layout(int cx, int ty, int tz, int bpt, int kf) {  // kf: flat nodes per thread
+    g_cx_override = cx; g_TY = ty; g_TZ = tz; g_BPT = bpt; g_KF = kf;
+}
+int or_apply_cx(int N) { return apply_cx(N); }
 
 int or_set_threads(int n) {
 #ifdef _OPENMP
@@ -693,8 +753,8 @@ int or_run_case(void* h, int n_steps, int snap_every, int max_iter, double tol,
             if (ref_snaps) {
                 const double* a = T;
                 const double* bb = ref_snaps + (size_t)si * Nn;
-                double num = o->creduce([&](long n, double acc) { double d = a[n] - bb[n]; return std::fma(d, d, acc); });
-                double den = o->creduce([&](long n, double acc) { return std::fma(bb[n], bb[n], acc); });
+                double num = o->freduce([&](long n, double acc) { double d = a[n] - bb[n]; return std::fma(d, d, acc); });
+                double den = o->freduce([&](long n, double acc) { return std::fma(bb[n], bb[n], acc); });
                 double dmax = 0.0;
                 for (long n = 0; n < Nn; ++n) { double d = std::fabs(a[n] - bb[n]); if (d > dmax) dmax = d; }
                 long cnt = 0;

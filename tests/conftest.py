@@ -25,6 +25,6 @@ def oracle():
     from oracle import oracle as om
     from mnhack8_b200 import _lib
 
-    lay = _lib.layout()
-    om.set_layout(lay["cx"], lay["ty"], lay["tz"], lay["bpt"])
+    lay = _lib.layout(128)
+    om.set_layout(0, lay["ty"], lay["tz"], lay["bpt"], lay["kf"])   # cx 0: per-N choice, as the library
     return om

@@ -29,10 +29,14 @@ def test_header_symbols_exported():
 
 
 def test_api_version_and_layout(oracle):
+    """The library's canonical reduction orders are the oracle's, for every grid size."""
     assert _lib.lib().hs_api_version() == 1
-    lay = _lib.layout()
+    lay = _lib.layout(128)
     assert lay["rt"] == 256 and lay["ty"] * lay["tz"] == 256
-    assert (lay["cx"], lay["ty"], lay["tz"], lay["bpt"]) == (16, 8, 32, 8)
+    assert (lay["ty"], lay["tz"], lay["bpt"], lay["kf"]) == (8, 32, 8, 2)
+    for N in range(1, 1201):
+        assert _lib.layout(N)["cx"] == oracle.apply_cx(N), N
+        assert 8 <= _lib.layout(N)["cx"] <= 64
 
 
 def test_no_oracle_in_library():
