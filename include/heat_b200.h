@@ -196,6 +196,21 @@ typedef struct hs_twin_summary {
 hs_status hs_classify(const hs_step_record* A, const hs_step_record* B, const hs_step_record* F, int n_steps,
                       int fi_level, int F_nonfinite, double dt, double thr_user, int detect, hs_twin_summary* out);
 
+/* x.y over the (N+1)^3 nodes of an N-element grid without allocating any
+ * device memory.  No counterpart in the reference.  For callers that cannot
+ * call cudaMalloc (a host application that owns the device-memory budget, a
+ * path that must not take the allocator's locks): the result equals hs_dot's
+ * bit for bit (same fixed reduction order), but the per-block partial sums
+ * live in a static device array of 65536 doubles (512 KiB, held by every GPU
+ * that loads the library until exit), so N <= 321 ((N+1)^3 <= 33554432 nodes);
+ * larger grids return HS_ERR_ARG.  x, y and out (one double) are device
+ * pointers on the current device; the work is enqueued on the default stream
+ * and *out is valid once that stream has completed.  The first call on a
+ * device looks up the array's device address and should come before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU
+ * race. */
+hs_status hs_dot_noalloc(int N, const double* x, const double* y, double* out);
+
 /* The reference solver's command line (het.cu:1340-1350, 1380-1433) with its
  * output files; returns the process exit code. */
 int hs_cli_main(int argc, char** argv);

@@ -25,7 +25,7 @@ EXPORTS = [
     "hs_destroy", "hs_num_nodes", "hs_field_stats", "hs_apply", "hs_precond", "hs_build_rhs", "hs_dot", "hs_pcg",
     "hs_arm_fi", "hs_run_case", "hs_verify", "hs_solve_host", "hs_diag_cg", "hs_set_dump", "hs_set_case_tag",
     "hs_target_on_boundary", "hs_classify", "hs_cli_main", "hs_advance", "hs_set_field", "hs_get_field",
-    "hs_time_kernel",
+    "hs_time_kernel", "hs_dot_noalloc",
 ]
 
 
@@ -130,6 +130,8 @@ def lib():
     L.hs_get_field.argtypes = [vp, vp]
     L.hs_time_kernel.restype = i
     L.hs_time_kernel.argtypes = [vp, i, i, pd]
+    L.hs_dot_noalloc.restype = i
+    L.hs_dot_noalloc.argtypes = [i, vp, vp, vp]
     L.hs_cli_main.restype = i
     L.hs_cli_main.argtypes = [i, C.POINTER(C.c_char_p)]
     _lib = L
@@ -322,6 +324,11 @@ def classify(A, B, F, fi_level, dt, thr_user=1e-13, detect=False, F_nonfinite=0)
                             int(detect), C.byref(out)))
     return {name: (getattr(out, name).decode() if name in ("cls", "detected_by") else getattr(out, name))
             for name, _ in TwinSummary._fields_ if name != "pad"}
+
+
+def dot_noalloc(N, x_dev, y_dev, out_dev):
+    """hs_dot_noalloc: x.y into the device double at out_dev, no device allocation."""
+    check(lib().hs_dot_noalloc(int(N), x_dev, y_dev, out_dev))
 
 
 def cli(argv):

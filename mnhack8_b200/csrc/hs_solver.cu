@@ -1021,3 +1021,6 @@ hs_status hs_time_kernel(hs_solver* h, int which, int reps, double* ms_per_launc
 }
 
 }  // extern "C"
+
+// the allocation-free dot product shares this translation unit's kernels
+#include "hs_noalloc.cu"
