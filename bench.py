@@ -86,6 +86,19 @@ def workload_config(args, world):
     }
 
 
+def reduce_over_ranks(dist, elapsed, iters, device):
+    """Replica aggregation: the slowest rank's elapsed time and all ranks' CG
+    iterations (every rank calls the same two collectives in the same order)."""
+    import torch
+    t = torch.tensor([float(elapsed), float(iters)], dtype=torch.float64, device=device)
+    if dist is not None:
+        tmax, tsum = t[0:1].clone(), t[1:2].clone()
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
+        return float(tmax[0]), float(tsum[0])
+    return float(t[0]), float(t[1])
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -271,13 +284,7 @@ def main():
         barrier()
     clocks = sampler.summary()
     # slowest rank's device time, all ranks' work
-    t = torch.tensor([tot_ms, float(tot_it)], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        tmax = t.clone()
-        dist.all_reduce(tmax[0:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(tmax[1:2], op=dist.ReduceOp.SUM)
-        t = tmax
-    ms_total, it_all = float(t[0]), float(t[1])
+    ms_total, it_all = reduce_over_ranks(dist, tot_ms, tot_it, "cuda")
     value = nodes * it_all / (ms_total * 1e-3)
     if args.profile:
         if rank == 0:
@@ -298,11 +305,8 @@ def main():
         it, _ = g.solve_host_ptr(T0.data_ptr(), Tout.data_ptr(), STEPS_PER_TRAJ)
         e2e_it += it
     e2e_s = time.perf_counter() - t0
-    te = torch.tensor([e2e_s, float(e2e_it)], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        dist.all_reduce(te[0:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(te[1:2], op=dist.ReduceOp.SUM)
-    e2e_value = nodes * float(te[1]) / float(te[0])
+    e2e_all_s, e2e_it_all = reduce_over_ranks(dist, e2e_s, e2e_it, "cuda")
+    e2e_value = nodes * e2e_it_all / e2e_all_s
 
     # ---- roofline of the dominant kernel (the fused PCG operator kernel) ----------
     ms_k1 = g.time_kernel(0, reps=20)
