@@ -110,7 +110,7 @@ def peaks():
 
 def profile_traffic(N):
     """dram bytes per launch of the PCG operator kernel from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", f"k_apply_colored_loop_N{N}.md")
+    p = os.path.join(ROOT, "profiles", f"k_apply_slab_loop_N{N}.md")
     if not os.path.exists(p):
         return None
     for line in open(p):
@@ -319,10 +319,10 @@ def main():
     traffic = profile_traffic(N)
     iters_per_traj = it_all / max(1, world) / args.steps
     # per time step: step begin/end, RHS and x0 operator (+ final each with ABFT),
-    # PCG prologue (update + final); per CG iteration: operator tiles + boundary
-    # + final, update + final
-    per_step = (2 + 2 * (3 if detect else 2) + 2) if args.scatter == "colored" else 12
-    per_iter = 5 if args.scatter == "colored" else 6
+    # PCG prologue (update + final); per CG iteration: operator + final,
+    # update + final
+    per_step = (2 + 2 * (2 if detect else 1) + 2) if args.scatter == "colored" else 12
+    per_iter = 4 if args.scatter == "colored" else 6
     launches = int(round(args.steps * (STEPS_PER_TRAJ * per_step + per_iter * iters_per_traj)))
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
@@ -332,7 +332,7 @@ def main():
         "config": workload_config(args, world),
         "cg_iters_per_trajectory": iters_per_traj,
         "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                     "traffic": traffic, "kernel": "k_apply_colored (PCG operator: p = z + beta p, Ap = A p, "
+                     "traffic": traffic, "kernel": "k_apply_slab (PCG operator: p = z + beta p, Ap = A p, "
                      "p.Ap and ABFT partials)", "alg_bytes_per_launch": alg_k1, "ms_per_launch": ms_k1,
                      "peak_source": f"{peak_kind} hbm_gbs", "l2": "flushed before each timed launch",
                      "update_kernel": {"ms_per_launch": ms_k2, "alg_bytes_per_launch": alg_k2,

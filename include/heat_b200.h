@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define HS_API_VERSION 1
+#define HS_API_VERSION 2
 
 typedef struct hs_solver hs_solver;
 
@@ -93,9 +93,9 @@ typedef struct hs_step_record {
     double solve_ms;    /* build_rhs + PCG (+ reprojection) device time of the step */
 } hs_step_record;
 
-/* canonical reduction orders of an N-element grid: the operator's tile
- * (planes cx, rows ty, columns tz; rt threads; bpt boundary nodes per thread)
- * and the flat order's nodes per thread kf */
+/* canonical reduction orders of an N-element grid: the operator's slab tile
+ * (planes cx, rows ty, columns tz; rt threads of bpt positions each, halo
+ * included) and the flat order's nodes per thread kf */
 typedef struct hs_layout_info { int cx, ty, tz, rt, bpt, kf; } hs_layout_info;
 
 void        hs_default_options(hs_options* opt);
@@ -120,7 +120,8 @@ hs_status hs_field_stats(const hs_solver* s, double out9[9]);
 /* y = (M + dt_eff K) x [+ Dirichlet projection] (apply_operator, het.cu:885-921).
  * allow_fi: a fault armed by hs_arm_fi (level R) fires in this call.
  * abft_rel (nullable): D1 relative checksum error when the handle has
- * detect on and project != 0, else -1. x, y: device. */
+ * detect on and project != 0, else -1. x, y: device, not overlapping
+ * (HS_ERR_ARG otherwise). */
 hs_status hs_apply(hs_solver* s, const double* x, double* y, double dt_eff, int allow_fi, int project,
                    double* abft_rel);
 /* z = r / diag (apply_preconditioner, het.cu:957-960). device. */

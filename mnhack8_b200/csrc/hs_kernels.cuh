@@ -23,6 +23,8 @@ struct ElemConsts {
 
 // local node i <-> q = ox<<2 | oy<<1 | oz   (het.cu:261-264)
 __device__ __constant__ int kQofLocal[8] = {0, 4, 6, 2, 1, 5, 7, 3};
+// canonical node sum: the corner q of each contributing element, in order
+__device__ __constant__ int kSumOrder[8] = {4, 7, 6, 5, 0, 3, 2, 1};
 
 __device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
@@ -119,47 +121,28 @@ __device__ __forceinline__ void elem_apply(double* v, double rhoc, double kc, do
 }
 
 // ---- partition helpers --------------------------------------------------------
-// apply partition of an N-element grid (cx planes per tile)
+// slab partition of an N-element grid (operator tiles) and the flat partition
 struct Part {
-    int N, NN, I, cx;
-    int NTX, NTY, NTZ, pad;
-    long long ntiles, NB, nbb, nblk;
+    int N, NN;
+    int C, R, CX;                     // tile columns, rows, planes
+    int Cw, Rw;                       // positions per row and rows per plane (halo included)
+    int NCB, NRB, NXB;                // tiles per direction (z, y, x)
+    long long ntiles, nblk;           // tiles = apply partials per quantity
     long long Nn, nflat;              // flat partition: blocks of RT*KF nodes
 };
 
-__host__ __device__ inline Part make_part(int N, int cx) {
-    Part p;
-    p.N = N; p.NN = N + 1; p.I = N - 1; p.cx = cx; p.pad = 0;
-    if (p.I > 0) {
-        p.NTX = (p.I + cx - 1) / cx; p.NTY = (p.I + TY - 1) / TY; p.NTZ = (p.I + TZ - 1) / TZ;
-        p.ntiles = (long long)p.NTX * p.NTY * p.NTZ;
-    } else {
-        p.NTX = p.NTY = p.NTZ = 0; p.ntiles = 0;
-    }
-    long long NN = p.NN;
+inline Part make_part(int N) {
+    Part p{};
+    const SlabLayout L = slab_layout(N);
+    p.N = N; p.NN = N + 1;
+    p.C = L.C; p.R = L.R; p.CX = L.CX;
+    p.Cw = L.C + 2; p.Rw = L.R + 2;
+    p.NCB = L.NCB; p.NRB = L.NRB; p.NXB = L.NXB;
+    p.ntiles = L.ntiles; p.nblk = L.ntiles;
+    const long long NN = p.NN;
     p.Nn = NN * NN * NN;
-    p.NB = p.Nn - (long long)p.I * p.I * p.I;
-    p.nbb = (p.NB + (long long)RT * BPT - 1) / ((long long)RT * BPT);
-    p.nblk = p.ntiles + p.nbb;
     p.nflat = (p.Nn + (long long)RT * KF - 1) / ((long long)RT * KF);
     return p;
-}
-
-// j-th boundary node in increasing node index
-__device__ __forceinline__ long long bnd_node(long long j, int N) {
-    const long long NN = N + 1, P = NN * NN;
-    if (j < P) return j;
-    long long jj = j - P;
-    const long long R = 4LL * N;
-    if (jj < (long long)(N - 1) * R) {
-        long long ix = 1 + jj / R, r = jj % R, iy, iz;
-        if (r < NN) { iy = 0; iz = r; }
-        else if (r < NN + 2LL * (N - 1)) { long long t = r - NN; iy = 1 + t / 2; iz = (t & 1) ? N : 0; }
-        else { iy = N; iz = r - NN - 2LL * (N - 1); }
-        return (ix * NN + iy) * NN + iz;
-    }
-    jj -= (long long)(N - 1) * R;
-    return (long long)N * P + jj;
 }
 
 __device__ __forceinline__ bool is_bnd(long long n, int N) {
@@ -167,6 +150,50 @@ __device__ __forceinline__ bool is_bnd(long long n, int N) {
     int ix = (int)(n / (NN * NN)), iy = (int)((n / NN) % NN), iz = (int)(n % NN);
     return ix == 0 || ix == N || iy == 0 || iy == N || iz == 0 || iz == N;
 }
+
+// tile t of the slab partition: first row y0, first column z0, planes xa..xb
+struct SlabTile { int y0, z0, xa, xb; };
+__device__ __forceinline__ SlabTile slab_tile(const Part& P, long long t) {
+    const int cb = (int)(t % P.NCB), rb = (int)((t / P.NCB) % P.NRB), tx = (int)(t / ((long long)P.NCB * P.NRB));
+    SlabTile s;
+    s.y0 = rb * P.R; s.z0 = cb * P.C; s.xa = tx * P.CX;
+    s.xb = min(s.xa + P.CX, P.NN) - 1;
+    return s;
+}
+
+// geometry of the SK positions of this thread in a slab CTA.  flags: bit k
+// node exists, bit 8+k element (lower corner at the position) exists, bit 16+k
+// tile node (output), bit 24+k on a y or z boundary face.
+struct SlabPos {
+    int noff[SK];     // node offset within a plane
+    int eoff[SK];     // element offset within an element layer
+    unsigned fl;
+};
+__device__ __forceinline__ SlabPos slab_pos(const Part& P, const SlabTile& T, int tid) {
+    SlabPos s;
+    s.fl = 0u;
+    const int N = P.N;
+#pragma unroll
+    for (int k = 0; k < SK; ++k) {
+        const int j = tid + k * ST;
+        const int lr = j / P.Cw, lc = j - lr * P.Cw;
+        const int gy = T.y0 - 1 + lr, gz = T.z0 - 1 + lc;
+        const bool in = j < P.Rw * P.Cw;
+        const bool valid = in && gy >= 0 && gy <= N && gz >= 0 && gz <= N;
+        const bool elem = in && lr <= P.Rw - 2 && lc <= P.Cw - 2 && gy >= 0 && gy < N && gz >= 0 && gz < N;
+        const bool out = valid && lr >= 1 && lr <= P.Rw - 2 && lc >= 1 && lc <= P.Cw - 2;
+        const bool yzb = gy == 0 || gy == N || gz == 0 || gz == N;
+        s.noff[k] = valid ? gy * P.NN + gz : 0;
+        s.eoff[k] = elem ? gy * N + gz : 0;
+        s.fl |= (valid ? 1u : 0u) << k | (elem ? 1u : 0u) << (8 + k) | (out ? 1u : 0u) << (16 + k) |
+                (yzb ? 1u : 0u) << (24 + k);
+    }
+    return s;
+}
+__device__ __forceinline__ bool sp_valid(unsigned fl, int k) { return (fl >> k) & 1u; }
+__device__ __forceinline__ bool sp_elem(unsigned fl, int k) { return (fl >> (8 + k)) & 1u; }
+__device__ __forceinline__ bool sp_out(unsigned fl, int k) { return (fl >> (16 + k)) & 1u; }
+__device__ __forceinline__ bool sp_yzb(unsigned fl, int k) { return (fl >> (24 + k)) & 1u; }
 
 // ---- canonical CTA tree ----------------------------------------------------------
 // sum over the RT threads of the CTA: xor butterfly inside each warp, then an
@@ -218,35 +245,6 @@ __device__ __forceinline__ void cta_tree_minmax(double& mn, double& mx, double (
     }
 }
 
-// Write the CTA partials, take a ticket; returns true in the last CTA, which
-// then holds the final canonical sums in v (thread 0).
-template <int NQ>
-__device__ __forceinline__ bool reduce_partials(double (&v)[NQ], double* partials, unsigned* ticket,
-                                                long long nblk, double (*sh)[8]) {
-    __shared__ unsigned s_last;
-    cta_tree_sum<NQ>(v, sh);
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int q = 0; q < NQ; ++q) partials[q * nblk + blockIdx.x] = v[q];
-        __threadfence();
-        unsigned t = atomicAdd(ticket, 1u);
-        s_last = (t == (unsigned)(nblk - 1));
-    }
-    __syncthreads();
-    if (!s_last) return false;
-    __threadfence();
-#pragma unroll
-    for (int q = 0; q < NQ; ++q) {
-        double acc = 0.0;
-        if (threadIdx.x < RT)
-            for (long long k = threadIdx.x; k < nblk; k += RT) acc = dadd(acc, __ldcg(partials + q * nblk + k));
-        v[q] = acc;
-    }
-    cta_tree_sum<NQ>(v, sh);
-    if (threadIdx.x == 0) *ticket = 0u;
-    return true;
-}
-
 // Combine the CTA's RT values (canonical tree) and store them as partial
 // blockIdx.x of each quantity; the reduction is finished by a final kernel.
 template <int NQ>
@@ -288,287 +286,174 @@ struct ApplyArgs {
     int d1;                 // evaluate the D1 checksum
     int pad1;
     double* partials;
-    unsigned* ticket;
     DevState* st;
     ElemConsts ec;
 };
 
-// cp.async (LDGSTS) 8-byte copies into shared memory; src-size 0 zero-fills
-__device__ __forceinline__ void cp_async8(void* smem, const double* gmem, bool pred) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    const int sz = pred ? 8 : 0;
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(sz) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int NPEND>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(NPEND) : "memory"); }
-
-// ---- colored operator, interior tiles: z-paired elements ----------------------
-// A CTA of KT = 160 threads handles one TY x TZ tile of node columns streaming
-// cx planes in x.  Element-pair thread p (< NPAIR) applies the two
-// z-adjacent elements (ley, 2j) and (ley, 2j+1) of each plane, which share
-// their common face; node-pair thread p (< NNPAIR) sums the contributions of
-// node columns (ly, 2j) and (ly, 2j+1) in the canonical order (lower x-plane
-// first, then (y, z)).  Node planes stream through a RING of shared-memory
-// slots filled by cp.async, AHEAD planes in flight.
-constexpr int KT = 160;
-constexpr int PZ = TZ / 2 + 1;        // element pairs per row (the last one half outside the tile)
-constexpr int NPAIR = EY * PZ;        // 153 element-pair threads
-constexpr int NNPAIR = TY * TZ / 2;   // 128 node-pair threads
-constexpr int LZ2 = 2 * PZ + 2;       // 36 node columns per loaded row (35 used, 16-byte rows)
-constexpr int NL2 = LY * LZ2;         // 360 node values per loaded plane
-constexpr int RING = 4;
-constexpr int AHEAD = RING - 2;
-static_assert(NPAIR <= KT && NNPAIR <= KT && KT % 32 == 0, "operator kernel thread count");
-static_assert(TZ % 2 == 0 && TY * TZ == RT && TZ / 2 == 16, "pair layout: 16 node pairs per row (half a warp)");
-struct __align__(16) ApplySmem {
-    double raw_a[RING][NL2];    // x, or z in the PCG loop (cp.async ring)
-    double raw_b[RING][NL2];    // p_{k-1} in the PCG loop
-    double pf[2][NL2];          // formed input planes p (PCG loop)
-    double2 yes[8][NPAIR];      // (element A, element B) outputs of each pair, by q
+// ---- colored operator: slab tiles ------------------------------------------------
+// One CTA of ST threads streams a tile's node planes in increasing x.  Per
+// element layer ix (between planes ix and ix+1):
+//   1. plane ix+1 is formed (p = z + beta p_{k-1} in the PCG loop) from
+//      registers loaded one layer ahead, kept in registers and published to
+//      shared memory;
+//   2. the element whose lower corner is a position (own column) gathers its
+//      six other corners from the two published planes, applies the element
+//      operator, folds its own-column outputs (q = 0 into the plane-ix node,
+//      q = 4 into the plane-(ix+1) node) into per-position accumulators and
+//      hands the other six to the three neighbouring positions;
+//   3. each tile node of plane ix adds the three handed-in contributions
+//      (q = 3, 2, 1), which completes its canonical node sum, and is
+//      projected, checked and stored; the plane-(ix+1) accumulators take
+//      q = 7, 6, 5.
+// Per node and layer that is one shared store of p, six shared loads for the
+// gather and three 16-byte stores and loads for the hand-over.
+struct __align__(16) SlabSmem {
+    double P[2][SPOS];      // formed planes, plane px in P[px & 1]
+    double2 Y1[SPOS];       // from the element at position j-1:      (q1, q5)
+    double2 Y2[SPOS];       // from the element at position j-Cw:     (q2, q6)
+    double2 Y3[SPOS];       // from the element at position j-Cw-1:   (q3, q7)
     double sh[MAXQ][8];
 };
-constexpr size_t kApplySmem = sizeof(ApplySmem);
-
-__device__ __forceinline__ double2 lds2(const double* p) { return *reinterpret_cast<const double2*>(p); }
+constexpr size_t kSlabSmem = sizeof(SlabSmem);
 
 // MODE 0: input x as given; 1: PCG loop, p = z; 2: PCG loop, p = z + beta p_{k-1}
 template <int FORM, int MODE>
-__device__ __forceinline__ void apply_tile_pairs(const ApplyArgs& a, ApplySmem& S, int N, int xa, int xb, int y0,
-                                                 int z0, const double* src_a, const double* src_b, double beta,
-                                                 double* pout, bool loop, bool d1, bool rhs, int fi_p, int fi_ap,
-                                                 int fi_r, int fi_bit, long long fi_idx, long long fi_elem,
-                                                 double (&pa)[MAXQ], double (&pb)[MAXQ]) {
-    constexpr bool FORMED = MODE > 0;
+__device__ __forceinline__ void slab_march(const ApplyArgs& a, SlabSmem& S, const SlabTile& T, const SlabPos& G,
+                                           const double* src_a, const double* src_b, double beta, double* pout,
+                                           bool loop, bool d1, bool rhs, int fi_p, int fi_ap, int fi_r, int fi_bit,
+                                           long long fi_idx, long long fi_elem, double (&part)[MAXQ]) {
     constexpr bool TWO = MODE == 2;
-    const int tid = threadIdx.x;
-    const int NN = N + 1;
-    const int plane = NN * NN, eplane = N * N;
-    // ---- copy slots: t, t + KT, t + 2 KT (< NL2) of a LY x LZ2 halo plane
-    int coff[3];
-    bool cok[3], chas[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const int sl = tid + k * KT;
-        chas[k] = sl < NL2;
-        const int row = sl / LZ2, col = sl % LZ2;
-        const int gy = y0 - 1 + row, gz = z0 - 1 + col;
-        cok[k] = chas[k] && col < LZ2 - 1 && gy <= N && gz <= N;
-        coff[k] = cok[k] ? gy * NN + gz : 0;
-    }
-    // ---- element pair
-    const bool has_e = tid < NPAIR;
-    const int ley = tid / PZ, jp = tid % PZ;
-    const int ey = y0 - 1 + ley, ez = z0 - 1 + 2 * jp;          // first element of the pair
-    const bool einA = has_e && ey <= N - 1 && ez <= N - 1;
-    const bool einB = has_e && ey <= N - 1 && ez + 1 <= N - 1;
-    const int eoA = einA ? ey * N + ez : 0;
-    const int eoB = einB ? ey * N + ez + 1 : 0;
-    const int elo = ley * LZ2 + 2 * jp;                          // node (ey, ez) in a halo plane
-    // ---- node pair
-    const bool has_n = tid < NNPAIR;
-    const int ly = tid / (TZ / 2), jn = tid % (TZ / 2);
-    const int iy = y0 + ly, iz = z0 + 2 * jn;
-    const bool nokA = has_n && iy <= N - 1 && iz <= N - 1;
-    const bool nokB = has_n && iy <= N - 1 && iz + 1 <= N - 1;
-    const int woff = iy * NN + iz;
-    const int pr0 = ly * PZ + jn, pr1 = (ly + 1) * PZ + jn;      // pairs (iy-1, .) and (iy, .) in yes[]
-    const int cidx = (ly + 1) * LZ2 + 2 * jn + 1;                // node (iy, iz) in a halo plane
-
-    int next_plane = xa - 1, next_base = (xa - 1) * plane;
-    auto issue_plane = [&]() {
-        if (next_plane <= xb + 1) {
-            const int slot = (next_plane - (xa - 1)) & (RING - 1);
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                if (chas[k]) {
-                    cp_async8(&S.raw_a[slot][tid + k * KT], src_a + (next_base + coff[k]), cok[k]);
-                    if (TWO) cp_async8(&S.raw_b[slot][tid + k * KT], src_b + (next_base + coff[k]), cok[k]);
-                }
-            }
-        }
-        cp_async_commit();
-        next_base += plane;
-        ++next_plane;
-    };
-    // p = z (+ beta p_{k-1}) for the copy slots of node plane px (ring slot rs)
-    auto form_plane = [&](int px, int rs) {
-        double* dst = S.pf[px & 1];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            if (chas[k]) {
-                const int sl = tid + k * KT;
-                double p = TWO ? dfma(beta, S.raw_b[rs][sl], S.raw_a[rs][sl]) : S.raw_a[rs][sl];
-                if (fi_p && cok[k] && (long long)px * plane + coff[k] == fi_idx) p = flipbit(p, fi_bit);
-                dst[sl] = p;
-            }
-        }
-    };
-    // coefficients of element plane ix, prefetched one plane ahead
-    int eb = (xa - 1) * eplane;
-    double rA = 0, kA = 0, rB = 0, kB = 0;
-    if (einA) { rA = __ldg(a.rhoc + eb + eoA); kA = __ldg(a.kc + eb + eoA); }
-    if (einB) { rB = __ldg(a.rhoc + eb + eoB); kB = __ldg(a.kc + eb + eoB); }
-    int nb = xa * plane + woff;      // node index of (ix, iy, iz) in the node phase
-    double wA = 0, wB = 0;
-    if (d1) { if (nokA) wA = __ldg(a.w + nb); if (nokB) wB = __ldg(a.w + nb + 1); }
-
-    for (int k = 0; k <= AHEAD; ++k) issue_plane();    // planes xa-1 .. xa+AHEAD-1
-    if (FORMED) {
-        cp_async_wait<AHEAD>();                         // plane xa-1
-        __syncthreads();
-        form_plane(xa - 1, 0);
-    }
-    double accA = 0.0, accB = 0.0;
-    for (int ix = xa - 1; ix <= xb; ++ix) {
-        const int lo = (ix - (xa - 1)) & (RING - 1);   // node plane ix
-        const int hi = (lo + 1) & (RING - 1);          // node plane ix+1
-        cp_async_wait<AHEAD - 1>();
-        __syncthreads();
-        issue_plane();
-        if (FORMED) {
-            form_plane(ix + 1, hi);
-            __syncthreads();
-        }
-        double rAn = 0, kAn = 0, rBn = 0, kBn = 0;     // element plane ix+1
-        if (ix + 1 <= xb) {
-            if (einA) { rAn = __ldg(a.rhoc + eb + eplane + eoA); kAn = __ldg(a.kc + eb + eplane + eoA); }
-            if (einB) { rBn = __ldg(a.rhoc + eb + eplane + eoB); kBn = __ldg(a.kc + eb + eplane + eoB); }
-        }
-        if (has_e) {
-            // 12 node values: columns c, c+1, c+2 of rows ley, ley+1 of planes ix, ix+1
-            double n_[2][2][3];
-#pragma unroll
-            for (int pl = 0; pl < 2; ++pl)
-#pragma unroll
-                for (int rw = 0; rw < 2; ++rw) {
-                    const double* src = FORMED ? &S.pf[(ix + pl) & 1][elo + rw * LZ2]
-                                               : &S.raw_a[pl ? hi : lo][elo + rw * LZ2];
-                    const double2 v01 = lds2(src);
-                    n_[pl][rw][0] = v01.x; n_[pl][rw][1] = v01.y; n_[pl][rw][2] = src[2];
-                }
-            double vA[8], vB[8];
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                vA[q] = n_[(q >> 2) & 1][(q >> 1) & 1][(q & 1)];
-                vB[q] = n_[(q >> 2) & 1][(q >> 1) & 1][1 + (q & 1)];
-            }
-            elem_apply<FORM>(vA, rA, kA, a.dt_eff, a.ec);
-            elem_apply<FORM>(vB, rB, kB, a.dt_eff, a.ec);
-            if (fi_r) {
-                if (einA && (long long)(eb + eoA) == fi_elem) vA[0] = flipbit(vA[0], fi_bit);
-                if (einB && (long long)(eb + eoB) == fi_elem) vB[0] = flipbit(vB[0], fi_bit);
-            }
-            // elements outside the domain (tile edges) produce garbage that no
-            // interior node reads
-#pragma unroll
-            for (int q = 0; q < 8; ++q) S.yes[q][tid] = make_double2(vA[q], vB[q]);
-        }
-        rA = rAn; kA = kAn; rB = rBn; kB = kBn;
-        eb += eplane;
-        __syncthreads();
-        if (has_n) {
-            // element pairs (iy-1 | iy, 2jn..2jn+1) by q; elements 2jn+1, 2jn+2 of
-            // the odd q come from this pair (.y) and the next pair (.x, from the
-            // next node-pair thread of the row, or loaded by the row's last one)
-            auto take = [&](int q, int pr, double& a_, double& b_, bool odd) {
-                const double2 v = S.yes[q][pr];
-                if (!odd) { a_ = v.x; b_ = v.y; return; }
-                double nxt = __shfl_down_sync(0xffffffffu, v.x, 1);
-                if (jn == TZ / 2 - 1) nxt = S.yes[q][pr + 1].x;
-                a_ = v.y; b_ = nxt;
-            };
-            if (ix >= xa) {
-                double c3a, c3b, c2a, c2b, c1a, c1b, c0a, c0b;
-                take(3, pr0, c3a, c3b, false);     // element (iy-1, iz-1) / (iy-1, iz)   for nodes A / B
-                take(2, pr0, c2a, c2b, true);      // element (iy-1, iz)   / (iy-1, iz+1)
-                take(1, pr1, c1a, c1b, false);     // element (iy,   iz-1) / (iy,   iz)
-                take(0, pr1, c0a, c0b, true);      // element (iy,   iz)   / (iy,   iz+1)
-                double yA = accA, yB = accB;
-                yA = dadd(yA, c3a); yA = dadd(yA, c2a); yA = dadd(yA, c1a); yA = dadd(yA, c0a);
-                yB = dadd(yB, c3b); yB = dadd(yB, c2b); yB = dadd(yB, c1b); yB = dadd(yB, c0b);
-                const double* cp_ = FORMED ? &S.pf[ix & 1][cidx] : &S.raw_a[lo][cidx];
-                const double pvA = cp_[0], pvB = cp_[1];
-                if (fi_ap) {
-                    if ((long long)nb == fi_idx) yA = flipbit(yA, fi_bit);
-                    if ((long long)nb + 1 == fi_idx) yB = flipbit(yB, fi_bit);
-                }
-                if (nokA) {
-                    if (loop) pa[0] = dfma(pvA, yA, pa[0]);
-                    if (d1) { pa[1] = dadd(pa[1], yA); pa[2] = dfma(wA, pvA, pa[2]); pa[3] = dfma(pvA, pvA, pa[3]); }
-                    if (rhs) yA = dfma(a.dtF, __ldg(a.F + nb), yA);
-                    a.y[nb] = yA;
-                    if (pout) pout[nb] = pvA;
-                }
-                if (nokB) {
-                    if (loop) pb[0] = dfma(pvB, yB, pb[0]);
-                    if (d1) { pb[1] = dadd(pb[1], yB); pb[2] = dfma(wB, pvB, pb[2]); pb[3] = dfma(pvB, pvB, pb[3]); }
-                    if (rhs) yB = dfma(a.dtF, __ldg(a.F + nb + 1), yB);
-                    a.y[nb + 1] = yB;
-                    if (pout) pout[nb + 1] = pvB;
-                }
-                nb += plane;
-                if (d1 && ix + 1 <= xb) {
-                    if (nokA) wA = __ldg(a.w + nb);
-                    if (nokB) wB = __ldg(a.w + nb + 1);
-                }
-            }
-            // contributions from below to the next node plane (ox = 1)
-            double c7a, c7b, c6a, c6b, c5a, c5b, c4a, c4b;
-            take(7, pr0, c7a, c7b, false);
-            take(6, pr0, c6a, c6b, true);
-            take(5, pr1, c5a, c5b, false);
-            take(4, pr1, c4a, c4b, true);
-            double nA = 0.0, nB = 0.0;
-            nA = dadd(nA, c7a); nA = dadd(nA, c6a); nA = dadd(nA, c5a); nA = dadd(nA, c4a);
-            nB = dadd(nB, c7b); nB = dadd(nB, c6b); nB = dadd(nB, c5b); nB = dadd(nB, c4b);
-            accA = nA; accB = nB;
-        }
-    }
-    cp_async_wait<0>();
-}
-
-// canonical tree of a tile whose node-pair thread p holds the column values
-// (ly, 2j) in va and (ly, 2j+1) in vb: the 32-lane butterfly of each row is a
-// 16-thread butterfly on both values (offsets 8..1 <-> column offsets 16..2)
-// followed by va + vb (column offset 1); rows are the canonical warps.
-template <int NQ>
-__device__ __forceinline__ void cta_tree_pairs(double (&va)[NQ], double (&vb)[NQ], double (*sh)[8]) {
-    const int tid = threadIdx.x;
-#pragma unroll
-    for (int q = 0; q < NQ; ++q) {
-#pragma unroll
-        for (int off = 8; off >= 1; off >>= 1) {
-            va[q] = dadd(va[q], __shfl_xor_sync(0xffffffffu, va[q], off));
-            vb[q] = dadd(vb[q], __shfl_xor_sync(0xffffffffu, vb[q], off));
-        }
-        va[q] = dadd(va[q], vb[q]);
-    }
-    __syncthreads();
-    if (tid < NNPAIR && (tid % (TZ / 2)) == 0) {
-#pragma unroll
-        for (int q = 0; q < NQ; ++q) sh[q][tid / (TZ / 2)] = va[q];
-    }
-    __syncthreads();
-    if (tid < 32) {
-        const int lane = tid;
-#pragma unroll
-        for (int q = 0; q < NQ; ++q) {
-            double u = (lane < 8) ? sh[q][lane] : 0.0;
-#pragma unroll
-            for (int off = 4; off >= 1; off >>= 1) u = dadd(u, __shfl_xor_sync(0xffffffffu, u, off));
-            va[q] = u;
-        }
-    }
-}
-
-// Colored operator, interior tiles (blocks 0 .. ntiles-1 of the apply partition).
-template <int FORM>
-__global__ void __launch_bounds__(KT, FORM == FORM_WHT ? 4 : 3) k_apply_colored(ApplyArgs a) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    ApplySmem& S = *reinterpret_cast<ApplySmem*>(smem_raw);
-    DevState* st = a.st;
     const Part& P = a.part;
+    const int N = P.N, Cw = P.Cw;
+    const long long plane = (long long)P.NN * P.NN, eplane = (long long)N * N;
+    const int tid = threadIdx.x;
+    const unsigned fl = G.fl;
+    const int xa = T.xa, xb = T.xb;
+
+    double pc[SK], pn[SK], ra[SK], rb[SK], cr[SK], ck[SK], wv[SK], fv[SK], acc[SK], accn[SK];
+    auto ld_raw = [&](int px) {
+        const bool pv = px >= 0 && px <= N;
+        const long long base = (long long)px * plane;
+#pragma unroll
+        for (int k = 0; k < SK; ++k) {
+            const bool v = pv && sp_valid(fl, k);
+            ra[k] = v ? __ldg(src_a + base + G.noff[k]) : 0.0;
+            if (TWO) rb[k] = v ? __ldg(src_b + base + G.noff[k]) : 0.0;
+        }
+    };
+    auto form = [&](int px, double (&p)[SK]) {
+        const long long base = (long long)px * plane;
+#pragma unroll
+        for (int k = 0; k < SK; ++k) {
+            double v = TWO ? dfma(beta, rb[k], ra[k]) : ra[k];
+            if (fi_p && sp_valid(fl, k) && base + G.noff[k] == fi_idx) v = flipbit(v, fi_bit);
+            p[k] = v;
+        }
+    };
+    auto ld_coef = [&](int ex) {
+        const bool ev = ex >= 0 && ex < N;
+        const long long base = (long long)ex * eplane;
+#pragma unroll
+        for (int k = 0; k < SK; ++k) {
+            const bool v = ev && sp_elem(fl, k);
+            cr[k] = v ? __ldg(a.rhoc + base + G.eoff[k]) : 0.0;
+            ck[k] = v ? __ldg(a.kc + base + G.eoff[k]) : 0.0;
+        }
+    };
+    auto ld_w = [&](int px) {
+        const bool pv = px >= xa && px <= xb;
+        const long long base = (long long)px * plane;
+#pragma unroll
+        for (int k = 0; k < SK; ++k) {
+            const bool v = pv && sp_out(fl, k);
+            wv[k] = (v && d1) ? __ldg(a.w + base + G.noff[k]) : 0.0;
+            if (MODE == 0) fv[k] = (v && rhs) ? __ldg(a.F + base + G.noff[k]) : 0.0;
+        }
+    };
+
+    // plane xa-1, then the inputs of plane xa and the coefficients of layer xa-1
+    ld_raw(xa - 1);
+    form(xa - 1, pc);
+#pragma unroll
+    for (int k = 0; k < SK; ++k) { S.P[(xa - 1) & 1][tid + k * ST] = pc[k]; acc[k] = 0.0; accn[k] = 0.0; }
+    ld_raw(xa);
+    ld_coef(xa - 1);
+
+    for (int ix = xa - 1; ix <= xb; ++ix) {
+        const int cur = ix & 1, nxt = (ix + 1) & 1;
+        // 1. plane ix+1
+        form(ix + 1, pn);
+#pragma unroll
+        for (int k = 0; k < SK; ++k) S.P[nxt][tid + k * ST] = pn[k];
+        ld_raw(ix + 2 <= xb + 1 ? ix + 2 : -2);
+        __syncthreads();
+        // 2. element layer ix
+        if (ix >= 0 && ix < N) {
+#pragma unroll
+            for (int k = 0; k < SK; ++k) {
+                if (!sp_elem(fl, k)) continue;
+                const int j = tid + k * ST;
+                double v[8];
+                v[0] = pc[k];
+                v[1] = S.P[cur][j + 1];
+                v[2] = S.P[cur][j + Cw];
+                v[3] = S.P[cur][j + Cw + 1];
+                v[4] = pn[k];
+                v[5] = S.P[nxt][j + 1];
+                v[6] = S.P[nxt][j + Cw];
+                v[7] = S.P[nxt][j + Cw + 1];
+                elem_apply<FORM>(v, cr[k], ck[k], a.dt_eff, a.ec);
+                if (fi_r && (long long)ix * eplane + G.eoff[k] == fi_elem) v[0] = flipbit(v[0], fi_bit);
+                acc[k] = dadd(acc[k], v[0]);
+                accn[k] = dadd(0.0, v[4]);
+                S.Y1[j + 1] = make_double2(v[1], v[5]);
+                S.Y2[j + Cw] = make_double2(v[2], v[6]);
+                S.Y3[j + Cw + 1] = make_double2(v[3], v[7]);
+            }
+        }
+        ld_coef(ix + 1 <= xb ? ix + 1 : -1);
+        __syncthreads();
+        // 3. tile nodes of plane ix; accumulators of plane ix+1
+        const long long base = (long long)ix * plane;
+        const bool xbnd = ix == 0 || ix == N;
+#pragma unroll
+        for (int k = 0; k < SK; ++k) {
+            if (!sp_out(fl, k)) continue;
+            const int j = tid + k * ST;
+            const bool yzin = !sp_yzb(fl, k);
+            double2 y3 = make_double2(0.0, 0.0), y2 = y3, y1 = y3;
+            if (yzin) { y3 = S.Y3[j]; y2 = S.Y2[j]; y1 = S.Y1[j]; }
+            if (ix >= xa) {
+                const long long n = base + G.noff[k];
+                const bool bnd = !yzin || xbnd;
+                double y = bnd ? 0.0 : dadd(dadd(dadd(acc[k], y3.x), y2.x), y1.x);
+                if (fi_ap && n == fi_idx) y = flipbit(y, fi_bit);
+                const double pv = pc[k];
+                if (loop) part[0] = dfma(pv, y, part[0]);
+                if (d1) {
+                    part[1] = bnd ? dfma(0.0, y, part[1]) : dadd(part[1], y);
+                    part[2] = dfma(wv[k], pv, part[2]);
+                    part[3] = dfma(pv, pv, part[3]);
+                }
+                if (MODE == 0 && rhs) y = dfma(a.dtF, fv[k], y);
+                a.y[n] = y;
+                if (TWO || MODE == 1) pout[n] = pv;
+            }
+            acc[k] = yzin ? dadd(dadd(dadd(accn[k], y3.y), y2.y), y1.y) : 0.0;
+        }
+        ld_w(ix + 1);
+#pragma unroll
+        for (int k = 0; k < SK; ++k) pc[k] = pn[k];
+    }
+}
+
+// Colored operator: tile blockIdx.x of the slab partition (every node of the
+// grid belongs to exactly one tile; boundary nodes are projected to zero).
+template <int FORM>
+__global__ void __launch_bounds__(ST, FORM == FORM_WHT ? 2 : 1) k_apply_slab(ApplyArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SlabSmem& S = *reinterpret_cast<SlabSmem*>(smem_raw);
+    DevState* st = a.st;
     const bool loop = a.role == ROLE_LOOP;
     int iter = 0;
     double beta = 0.0;
@@ -592,99 +477,20 @@ __global__ void __launch_bounds__(KT, FORM == FORM_WHT ? 4 : 3) k_apply_colored(
     }
     const bool d1 = a.d1 != 0;
     const bool rhs = (a.role == ROLE_RHS) && a.F != nullptr;
-    double pa[MAXQ] = {0.0, 0.0, 0.0, 0.0}, pb[MAXQ] = {0.0, 0.0, 0.0, 0.0};
-    const long long t = blockIdx.x;
-    const int tz = (int)(t % P.NTZ), ty = (int)((t / P.NTZ) % P.NTY), tx = (int)(t / ((long long)P.NTZ * P.NTY));
-    const int y0 = 1 + ty * TY, z0 = 1 + tz * TZ;
-    const int xa = 1 + tx * P.cx, xb = min(tx * P.cx + P.cx, P.I);
-    if (!loop)
-        apply_tile_pairs<FORM, 0>(a, S, a.N, xa, xb, y0, z0, src_a, src_b, beta, pout, loop, d1, rhs, fi_p, fi_ap,
-                                  fi_r, fi_bit, fi_idx, fi_elem, pa, pb);
-    else if (!src_b)
-        apply_tile_pairs<FORM, 1>(a, S, a.N, xa, xb, y0, z0, src_a, src_b, beta, pout, loop, d1, rhs, fi_p, fi_ap,
-                                  fi_r, fi_bit, fi_idx, fi_elem, pa, pb);
-    else
-        apply_tile_pairs<FORM, 2>(a, S, a.N, xa, xb, y0, z0, src_a, src_b, beta, pout, loop, d1, rhs, fi_p, fi_ap,
-                                  fi_r, fi_bit, fi_idx, fi_elem, pa, pb);
-    if (!loop && !d1) return;
-    cta_tree_pairs<MAXQ>(pa, pb, S.sh);
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int q = 0; q < MAXQ; ++q) a.partials[q * P.nblk + t] = pa[q];
-    }
-}
-
-// Colored operator, boundary nodes (blocks ntiles .. nblk-1 of the apply
-// partition; the projection makes their outputs zero): input formation, the
-// fault hooks, the partials and the stores.
-__global__ void __launch_bounds__(RT) k_apply_boundary(ApplyArgs a) {
-    __shared__ double sh[MAXQ][8];
-    DevState* st = a.st;
-    const Part& P = a.part;
-    const int N = a.N;
-    const int tid = threadIdx.x;
-    const bool loop = a.role == ROLE_LOOP;
-    int iter = 0;
-    double beta = 0.0;
-    const double* src_a = a.x;
-    const double* src_b = nullptr;
-    double* pout = nullptr;
-    int fi_p = 0, fi_ap = 0, fi_bit = 0;
-    long long fi_idx = -1;
-    if (loop) {
-        if (st->done) return;
-        iter = st->iter; beta = st->beta;
-        src_a = a.z;
-        src_b = (iter > 0) ? ((iter & 1) ? a.pbuf0 : a.pbuf1) : nullptr;
-        pout = (iter & 1) ? a.pbuf1 : a.pbuf0;
-        if (st->fi_vec && st->fi_iter == iter) {
-            fi_idx = st->fi_idx; fi_bit = st->fi_bit;
-            fi_p = (st->fi_vec == FI_P); fi_ap = (st->fi_vec == FI_AP);
-        }
-    }
-    const bool d1 = a.d1 != 0;
-    const bool rhs = (a.role == ROLE_RHS) && a.F != nullptr;
-    const bool two = src_b != nullptr;
     double part[MAXQ] = {0.0, 0.0, 0.0, 0.0};
-    const long long b = blockIdx.x;
-    long long nk[BPT];
-    double va[BPT], vb[BPT], wv[BPT];
-#pragma unroll
-    for (int k = 0; k < BPT; ++k) {
-        const long long j = b * (long long)(RT * BPT) + (long long)k * RT + tid;
-        nk[k] = (j < P.NB) ? bnd_node(j, N) : -1;
-    }
-#pragma unroll
-    for (int k = 0; k < BPT; ++k) {
-        const long long n = nk[k];
-        va[k] = (n >= 0) ? __ldg(src_a + n) : 0.0;
-        vb[k] = (n >= 0 && two) ? __ldg(src_b + n) : 0.0;
-        wv[k] = (n >= 0 && d1) ? __ldg(a.w + n) : 0.0;
-    }
-#pragma unroll
-    for (int k = 0; k < BPT; ++k) {
-        const long long n = nk[k];
-        if (n < 0) break;
-        double pv = two ? dfma(beta, vb[k], va[k]) : va[k];
-        if (fi_p && n == fi_idx) pv = flipbit(pv, fi_bit);
-        double yv = 0.0;
-        if (fi_ap && n == fi_idx) yv = flipbit(yv, fi_bit);
-        if (loop) part[0] = dfma(pv, yv, part[0]);
-        if (d1) {
-            part[1] = dfma(0.0, yv, part[1]);
-            part[2] = dfma(wv[k], pv, part[2]);
-            part[3] = dfma(pv, pv, part[3]);
-        }
-        if (rhs) yv = dfma(a.dtF, __ldg(a.F + n), yv);
-        a.y[n] = yv;
-        if (pout) pout[n] = pv;
-    }
+    const SlabTile T = slab_tile(a.part, blockIdx.x);
+    const SlabPos G = slab_pos(a.part, T, threadIdx.x);
+    if (!loop)
+        slab_march<FORM, 0>(a, S, T, G, src_a, src_b, beta, pout, loop, d1, rhs, fi_p, fi_ap, fi_r, fi_bit, fi_idx,
+                            fi_elem, part);
+    else if (!src_b)
+        slab_march<FORM, 1>(a, S, T, G, src_a, src_b, beta, pout, loop, d1, rhs, fi_p, fi_ap, fi_r, fi_bit, fi_idx,
+                            fi_elem, part);
+    else
+        slab_march<FORM, 2>(a, S, T, G, src_a, src_b, beta, pout, loop, d1, rhs, fi_p, fi_ap, fi_r, fi_bit, fi_idx,
+                            fi_elem, part);
     if (!loop && !d1) return;
-    cta_tree_sum<MAXQ>(part, sh);
-    if (tid == 0) {
-#pragma unroll
-        for (int q = 0; q < MAXQ; ++q) a.partials[q * P.nblk + P.ntiles + b] = part[q];
-    }
+    store_partials<MAXQ>(part, a.partials, a.part.nblk, S.sh);
 }
 
 // Role logic of an operator application once its partials are complete:
@@ -969,7 +775,7 @@ __global__ void k_absdiff_count(long long Nn, const double* a, const double* b, 
 
 // ---- node-parallel operator (every node, any projection) -------------------------
 // Recomputes the eight elements around each node; bit-identical node values to
-// k_apply_colored (same element arithmetic, same summation order).  Used for
+// k_apply_slab (same element arithmetic, same summation order).  Used for
 // the unprojected set-up applies and the diagonal.
 enum GenKind { GEN_APPLY = 0, GEN_DIAG = 1 };
 struct GenArgs {
@@ -995,11 +801,10 @@ __global__ void __launch_bounds__(RT) k_apply_nodes(GenArgs a) {
     double acc = 0.0;
 #pragma unroll 1
     for (int s = 0; s < 8; ++s) {
-        const int ao = (s >> 2) & 1, bo = (s >> 1) & 1, co = s & 1;
-        const int ex = ix - 1 + ao, ey = iy - 1 + bo, ez = iz - 1 + co;
+        const int qn = kSumOrder[s];
+        const int ex = ix - ((qn >> 2) & 1), ey = iy - ((qn >> 1) & 1), ez = iz - (qn & 1);
         if (ex < 0 || ey < 0 || ez < 0 || ex >= N || ey >= N || ez >= N) continue;
         const long long e = ((long long)ex * N + ey) * N + ez;
-        const int qn = ((1 - ao) << 2) | ((1 - bo) << 1) | (1 - co);
         double c;
         if (a.kind == GEN_DIAG) {
             const int i = (qn == 0) ? 0 : (qn == 4) ? 1 : (qn == 6) ? 2 : (qn == 2) ? 3 : (qn == 1) ? 4 : (qn == 5) ? 5 : (qn == 7) ? 6 : 7;
@@ -1076,13 +881,11 @@ struct FinishArgs {
     unsigned* ticket;
     DevState* st;
 };
-__global__ void __launch_bounds__(RT) k_finish_atomic(FinishArgs a) {
+__global__ void __launch_bounds__(ST) k_finish_atomic(FinishArgs a) {
     __shared__ double sh[MAXQ][8];
     DevState* st = a.st;
     const int N = a.N;
-    const long long NN = N + 1;
     const Part& P = a.part;
-    const int tid = threadIdx.x;
     int fi_ap = 0, fi_bit = 0;
     long long fi_idx = -1;
     int iter = 0;
@@ -1094,34 +897,27 @@ __global__ void __launch_bounds__(RT) k_finish_atomic(FinishArgs a) {
     const double* p = (a.role == ROLE_LOOP) ? ((iter & 1) ? a.pbuf1 : a.pbuf0) : a.p;
     const bool rhs = (a.role == ROLE_RHS) && a.F != nullptr;
     double part[MAXQ] = {0.0, 0.0, 0.0, 0.0};
-    auto node = [&](long long n, bool bnd) {
-        double yv = bnd ? 0.0 : a.y[n];
-        if (fi_ap && n == fi_idx) yv = flipbit(yv, fi_bit);
-        const double pv = __ldg(p + n);
-        if (a.role == ROLE_LOOP) part[0] = dfma(pv, yv, part[0]);
-        if (a.d1) {
-            part[1] = dfma(bnd ? 0.0 : 1.0, yv, part[1]);
-            part[2] = dfma(__ldg(a.w + n), pv, part[2]);
-            part[3] = dfma(pv, pv, part[3]);
-        }
-        if (rhs) yv = dfma(a.dtF, __ldg(a.F + n), yv);
-        a.y[n] = yv;
-    };
-    if (blockIdx.x < P.ntiles) {
-        const long long t = blockIdx.x;
-        const int tz = (int)(t % P.NTZ), ty = (int)((t / P.NTZ) % P.NTY), tx = (int)(t / ((long long)P.NTZ * P.NTY));
-        const int iy = 1 + ty * TY + tid / TZ, iz = 1 + tz * TZ + tid % TZ;
-        if (iy <= P.I && iz <= P.I) {
-            const int xa = 1 + tx * P.cx, xb = min(tx * P.cx + P.cx, P.I);
-            for (int ix = xa; ix <= xb; ++ix) node(((long long)ix * NN + iy) * NN + iz, false);
-        }
-    } else {
-        const long long b = blockIdx.x - P.ntiles;
-#pragma unroll 1
-        for (int k = 0; k < BPT; ++k) {
-            const long long j = b * (long long)(RT * BPT) + (long long)k * RT + tid;
-            if (j >= P.NB) break;
-            node(bnd_node(j, N), true);
+    const SlabTile T = slab_tile(P, blockIdx.x);
+    const SlabPos G = slab_pos(P, T, threadIdx.x);
+    const long long plane = (long long)P.NN * P.NN;
+    for (int ix = T.xa; ix <= T.xb; ++ix) {
+        const bool xbnd = ix == 0 || ix == N;
+#pragma unroll
+        for (int k = 0; k < SK; ++k) {
+            if (!sp_out(G.fl, k)) continue;
+            const long long n = (long long)ix * plane + G.noff[k];
+            const bool bnd = xbnd || sp_yzb(G.fl, k);
+            double yv = bnd ? 0.0 : a.y[n];
+            if (fi_ap && n == fi_idx) yv = flipbit(yv, fi_bit);
+            const double pv = __ldg(p + n);
+            if (a.role == ROLE_LOOP) part[0] = dfma(pv, yv, part[0]);
+            if (a.d1) {
+                part[1] = bnd ? dfma(0.0, yv, part[1]) : dadd(part[1], yv);
+                part[2] = dfma(__ldg(a.w + n), pv, part[2]);
+                part[3] = dfma(pv, pv, part[3]);
+            }
+            if (rhs) yv = dfma(a.dtF, __ldg(a.F + n), yv);
+            a.y[n] = yv;
         }
     }
     if (a.role != ROLE_LOOP && !a.d1) return;

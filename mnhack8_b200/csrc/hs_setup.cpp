@@ -161,14 +161,14 @@ void build_source(int N, double src_sigma, std::vector<double>& F) {
         for (long ix = a; ix < b; ++ix) {
             elem_plane((int)ix, hi);
             for (int iy = 1; iy < N; ++iy) for (int iz = 1; iz < N; ++iz) {
+                // canonical node sum: element corners q = 4, 7, 6, 5, 0, 3, 2, 1
+                static const int order[8] = {4, 7, 6, 5, 0, 3, 2, 1};
                 double acc = 0.0;
-                for (int pa = 0; pa < 2; ++pa) {
-                    const std::vector<double>& pl = pa ? hi : lo;
-                    for (int pb = 0; pb < 2; ++pb) for (int pc = 0; pc < 2; ++pc) {
-                        const int ey = iy - 1 + pb, ez = iz - 1 + pc;
-                        const int q = ((1 - pa) << 2) | ((1 - pb) << 1) | (1 - pc);
-                        acc = acc + pl[((size_t)ey * N + ez) * 8 + q];
-                    }
+                for (int s = 0; s < 8; ++s) {
+                    const int q = order[s];
+                    const std::vector<double>& pl = ((q >> 2) & 1) ? lo : hi;
+                    const int ey = iy - ((q >> 1) & 1), ez = iz - (q & 1);
+                    acc = acc + pl[((size_t)ey * N + ez) * 8 + q];
                 }
                 F[(ix * NN + iy) * NN + iz] = acc;
             }

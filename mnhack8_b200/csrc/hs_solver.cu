@@ -64,8 +64,6 @@ struct hs_solver {
     ElemConsts ec{};
     double kmin = 0, kmax = 0, rhocmin = 0, rhocmax = 0;
     cudaStream_t s = nullptr;
-    cudaStream_t s2 = nullptr;          // side stream: boundary-node kernels run beside the tiles
-    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
 
     DevBuf<double> rhoc, kc, gtab;
     DevBuf<double> diag, F, wM, wA;
@@ -101,9 +99,6 @@ struct hs_solver {
             if (graph[i]) cudaGraphDestroy(graph[i]);
         }
         for (double* q : ref_snaps) cudaFree(q);
-        if (fork_ev) cudaEventDestroy(fork_ev);
-        if (join_ev) cudaEventDestroy(join_ev);
-        if (s2) cudaStreamDestroy(s2);
         if (s) cudaStreamDestroy(s);
     }
 };
@@ -129,27 +124,19 @@ bool set_smem_attributes() {
     static bool done = false, ok = true;
     if (done) return ok;
     done = true;
-    ok = cudaFuncSetAttribute(k_apply_colored<FORM_WHT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kApplySmem) == cudaSuccess &&
-         cudaFuncSetAttribute(k_apply_colored<FORM_FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kApplySmem) == cudaSuccess &&
-         cudaFuncSetAttribute(k_apply_colored<FORM_GAUSS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kApplySmem) == cudaSuccess;
+    ok = cudaFuncSetAttribute(k_apply_slab<FORM_WHT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSlabSmem) == cudaSuccess &&
+         cudaFuncSetAttribute(k_apply_slab<FORM_FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSlabSmem) == cudaSuccess &&
+         cudaFuncSetAttribute(k_apply_slab<FORM_GAUSS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSlabSmem) == cudaSuccess;
     return ok;
 }
 
 void launch_colored(hs_solver* h, const ApplyArgs& a) {
     const int g = (int)h->part.ntiles;
-    // boundary nodes on the side stream, concurrently with the tiles
-    cudaEventRecord(h->fork_ev, h->s);
-    cudaStreamWaitEvent(h->s2, h->fork_ev, 0);
-    k_apply_boundary<<<(int)h->part.nbb, RT, 0, h->s2>>>(a);
-    cudaEventRecord(h->join_ev, h->s2);
-    if (g > 0) {
-        switch (h->opt.kernel) {
-            case HS_KERNEL_WHT: k_apply_colored<FORM_WHT><<<g, KT, kApplySmem, h->s>>>(a); break;
-            case HS_KERNEL_GAUSS: k_apply_colored<FORM_GAUSS><<<g, KT, kApplySmem, h->s>>>(a); break;
-            default: k_apply_colored<FORM_FAST><<<g, KT, kApplySmem, h->s>>>(a); break;
-        }
+    switch (h->opt.kernel) {
+        case HS_KERNEL_WHT: k_apply_slab<FORM_WHT><<<g, ST, kSlabSmem, h->s>>>(a); break;
+        case HS_KERNEL_GAUSS: k_apply_slab<FORM_GAUSS><<<g, ST, kSlabSmem, h->s>>>(a); break;
+        default: k_apply_slab<FORM_FAST><<<g, ST, kSlabSmem, h->s>>>(a); break;
     }
-    cudaStreamWaitEvent(h->s, h->join_ev, 0);
 }
 void launch_nodes(hs_solver* h, const GenArgs& a) {
     const int g = grid_for(h->Nn, RT, 1 << 30);
@@ -180,7 +167,7 @@ void apply_projected(hs_solver* h, int role, const double* x, double* y, double 
         a.x = x; a.z = h->z.p; a.pbuf0 = h->p0.p; a.pbuf1 = h->p1.p;
         a.y = y; a.rhoc = h->rhoc.p; a.kc = h->kc.p; a.w = w; a.F = F; a.dtF = dtF;
         a.d1 = d1 ? 1 : 0;
-        a.partials = h->partials.p; a.ticket = h->ticket.p; a.st = h->st.p; a.ec = h->ec;
+        a.partials = h->partials.p; a.st = h->st.p; a.ec = h->ec;
         launch_colored(h, a);
         if (role == ROLE_LOOP || d1) {
             FinalApplyArgs fa{h->partials.p, h->part.nblk, h->st.p, role, d1 ? 1 : 0};
@@ -202,7 +189,7 @@ void apply_projected(hs_solver* h, int role, const double* x, double* y, double 
     f.N = h->N; f.role = role; f.d1 = d1 ? 1 : 0; f.p = x; f.pbuf0 = h->p0.p; f.pbuf1 = h->p1.p;
     f.y = y; f.w = w; f.F = F; f.dtF = dtF;
     f.partials = h->partials.p; f.ticket = h->ticket.p; f.st = h->st.p;
-    k_finish_atomic<<<nblocks(h), RT, 0, h->s>>>(f);
+    k_finish_atomic<<<nblocks(h), ST, 0, h->s>>>(f);
     if (role == ROLE_LOOP || d1) {
         FinalApplyArgs fa{h->partials.p, h->part.nblk, h->st.p, role, d1 ? 1 : 0};
         k_final_apply<<<1, RT, 0, h->s>>>(fa);
@@ -323,7 +310,8 @@ const char* hs_last_error(void) { return hs::g_err.c_str(); }
 
 void hs_get_layout(int N, hs_layout_info* out) {
     if (!out) return;
-    out->cx = apply_cx(N); out->ty = TY; out->tz = TZ; out->rt = RT; out->bpt = BPT; out->kf = KF;
+    const SlabLayout L = slab_layout(N);
+    out->cx = L.CX; out->ty = L.R; out->tz = L.C; out->rt = RT; out->bpt = SK; out->kf = KF;
 }
 
 void hs_default_options(hs_options* o) {
@@ -386,7 +374,7 @@ hs_status hs_create(const hs_options* opt, const double* k_host, const double* r
     h->N = N;
     h->Nn = (long long)(N + 1) * (N + 1) * (N + 1);
     h->Ne = (long long)N * N * N;
-    h->part = make_part(N, apply_cx(N));
+    h->part = make_part(N);
     h->kmin = h->kmax = k_host[0];
     h->rhocmin = h->rhocmax = rhoc_host[0];
     for (long long e = 0; e < h->Ne; ++e) {
@@ -414,9 +402,6 @@ hs_status hs_create(const hs_options* opt, const double* k_host, const double* r
     h->ec.detJ = h->mats.detJ;
 
     HS_CUDA(cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking));
-    HS_CUDA(cudaStreamCreateWithFlags(&h->s2, cudaStreamNonBlocking));
-    HS_CUDA(cudaEventCreateWithFlags(&h->fork_ev, cudaEventDisableTiming));
-    HS_CUDA(cudaEventCreateWithFlags(&h->join_ev, cudaEventDisableTiming));
     const size_t Nn = (size_t)h->Nn, Ne = (size_t)h->Ne;
     HS_CUDA(h->rhoc.alloc(Ne)); HS_CUDA(h->kc.alloc(Ne)); HS_CUDA(h->gtab.alloc(256));
     HS_CUDA(h->diag.alloc(Nn)); HS_CUDA(h->F.alloc(Nn));
@@ -507,6 +492,11 @@ hs_status hs_arm_fi(hs_solver* s, const hs_fi_spec* fi) {
 
 hs_status hs_apply(hs_solver* s, const double* x, double* y, double dt_eff, int allow_fi, int project, double* abft_rel) {
     if (!s || !x || !y) { set_error("bad arguments"); return HS_ERR_ARG; }
+    if (x < y + s->Nn && y < x + s->Nn) {
+        // tiles read halo nodes of x that neighbouring tiles write in y
+        set_error("hs_apply: x and y overlap (the operator is not applied in place)");
+        return HS_ERR_ARG;
+    }
     if (abft_rel) *abft_rel = -1.0;
     StepCtl c{};
     if (allow_fi && s->pending_set && s->pending.level == HS_FI_R) {

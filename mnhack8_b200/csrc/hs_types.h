@@ -5,52 +5,77 @@
 namespace hs {
 
 // ---- canonical partitions and reduction orders ------------------------------
-// APPLY partition (operator kernels): interior nodes [1, N-1]^3 are covered by
-// tiles of TY rows x TZ columns streaming cx(N) planes in x, one node column
-// per reduction thread; boundary nodes (any coordinate 0 or N), enumerated in
-// increasing node index, by blocks of RT*BPT nodes, thread t taking nodes
-// b*RT*BPT + k*RT + t for k = 0..BPT-1.  The p.Ap and ABFT partials follow it.
+// SLAB partition (operator kernels and the p.Ap / ABFT partials): the node grid
+// is cut into tiles of CX planes (x) x R rows (y) x C columns (z) (the last
+// tile of each direction may be short).  Tile t = (tx * NRB + rb) * NCB + cb
+// covers planes [tx*CX, ..), rows [rb*R, ..), columns [cb*C, ..).  Its CTA
+// holds the tile's rows and columns plus a one-node halo on each side as
+// Rw = R+2 rows of Cw = C+2 positions, position j = lr*Cw + lc <-> node row
+// rb*R - 1 + lr, column cb*C - 1 + lc; thread t owns positions t + k*ST,
+// k = 0..SK-1.  A thread accumulates the tile nodes among its positions, plane
+// by plane in increasing x, positions in increasing k.
 // FLAT partition (every other reduction and the PCG vector update): blocks of
 // RT*KF consecutive nodes, thread t of block b taking the KF consecutive nodes
 // b*RT*KF + t*KF + k.
-// In both, a thread accumulates its nodes in order, a block combines its RT
-// values by a 32-lane xor butterfly per warp and an 8-way xor butterfly over
-// the warp sums, and the last block to finish combines the per-block partials
-// (apply: tiles first, then boundary blocks) by RT strided sequential sums and
-// the same block tree.  Every result is a fixed function of the inputs,
-// independent of scheduling.
-constexpr int TY = 8;
-constexpr int TZ = 32;
+// In both, a block combines its RT values by a 32-lane xor butterfly per warp
+// and an 8-way xor butterfly over the warp sums, and a final pass combines the
+// per-block partials by RT strided sequential sums and the same block tree.
+// Every result is a fixed function of the inputs, independent of scheduling.
+//
+// Node sums (operator output at a node): starting from +0.0, the contributions
+// of the elements around the node are added in the order of their local
+// corner q = ox<<2 | oy<<1 | oz at which the node sits: 4, 7, 6, 5, 0, 3, 2, 1
+// (the lower x layer first, each layer's own-column element first), skipping
+// elements outside the domain.
 constexpr int RT = 256;
-constexpr int BPT = 8;
 constexpr int KF = 2;
-constexpr int APPLY_SLOTS = 592;   // co-resident operator tiles assumed by cx(N): 148 SMs x 4
+constexpr int ST = RT;                // threads per slab CTA
+constexpr int SK = 4;                 // positions per thread
+constexpr int SPOS = ST * SK;         // positions per plane of a slab CTA (halo included)
+constexpr int SLAB_SLOTS = 296;       // co-resident slab CTAs assumed by the layout: 148 SMs x 2
 
-// planes per apply tile: the cx in [8, 64] minimising (waves x (cx + 1) element
-// planes) for APPLY_SLOTS co-resident tiles
-inline int apply_cx(int N) {
-    const long long I = N - 1;
-    if (I <= 0) return 16;
-    const long long col = ((I + TY - 1) / TY) * ((I + TZ - 1) / TZ);
-    int best = 16;
+struct SlabLayout {
+    int C, R, CX;          // tile columns, rows, planes
+    int NCB, NRB, NXB;     // tiles per direction
+    long long ntiles;
+};
+
+// The tile shape of an N-element grid: among C >= min(N+1, 30) with
+// (R+2)(C+2) <= SPOS (R as large as that allows) and CX from the first waves
+// of SLAB_SLOTS tiles, the one minimising waves x (CX+2) x
+// ((R+2)(C+2) + 2(R+1)(C+1)) (planes streamed x positions loaded plus twice
+// the elements applied per plane); ties keep the smaller C, then fewer waves.
+inline SlabLayout slab_layout(int N) {
+    const long long NN = N + 1;
+    SlabLayout best{};
     long long best_cost = -1;
-    for (int cx = 8; cx <= 64; ++cx) {
-        const long long chunks = (I + cx - 1) / cx;
-        const long long blocks = col * chunks;
-        const long long waves = (blocks + APPLY_SLOTS - 1) / APPLY_SLOTS;
-        const long long cost = waves * ((cx < I ? cx : I) + 1);
-        if (best_cost < 0 || cost < best_cost) { best_cost = cost; best = cx; }
+    const long long cmin = NN < 30 ? NN : 30;
+    for (long long C = cmin; C <= NN; ++C) {
+        const long long Cw = C + 2;
+        const long long Rmax = SPOS / Cw - 2;
+        if (Rmax < 1) break;
+        const long long R = Rmax < NN ? Rmax : NN;
+        const long long NCB = (NN + C - 1) / C, NRB = (NN + R - 1) / R, tyz = NCB * NRB;
+        const long long work = Cw * (R + 2) + 2 * (C + 1) * (R + 1);
+        const long long w0 = (tyz + SLAB_SLOTS - 1) / SLAB_SLOTS;
+        for (long long w = w0; w < w0 + 4; ++w) {
+            long long nx = w * SLAB_SLOTS / tyz;
+            if (nx < 1) continue;
+            if (nx > NN) nx = NN;
+            const long long CX = (NN + nx - 1) / nx;
+            const long long NXB = (NN + CX - 1) / CX;
+            const long long waves = (tyz * NXB + SLAB_SLOTS - 1) / SLAB_SLOTS;
+            const long long cost = waves * (CX + 2) * work;
+            if (best_cost < 0 || cost < best_cost) {
+                best_cost = cost;
+                best.C = (int)C; best.R = (int)R; best.CX = (int)CX;
+                best.NCB = (int)NCB; best.NRB = (int)NRB; best.NXB = (int)NXB;
+                best.ntiles = tyz * NXB;
+            }
+        }
     }
     return best;
 }
-constexpr int EY = TY + 1;            // element rows touched by a tile
-constexpr int EZ = TZ + 1;            // element columns touched by a tile
-constexpr int LY = TY + 2;            // node rows loaded per plane (with halo)
-constexpr int LZ = TZ + 2;            // node columns loaded per plane
-constexpr int NLOAD = LY * LZ;        // 340 node values per plane
-constexpr int NELEM = EY * EZ;        // 297 elements per plane
-static_assert(TY * TZ == RT, "one node column per thread");
-static_assert(NLOAD <= 2 * RT && NELEM <= 2 * RT, "two slots per thread");
 
 constexpr int MAXQ = 4;               // reduced quantities per pass
 

@@ -47,41 +47,67 @@ namespace {
 
 // ---- canonical reduction partitions (mirror the library's) --------------------
 // Two fixed orders.  The APPLY order (the operator kernel's p.Ap and ABFT
-// partials) follows the operator's tiles, described below.  The FLAT order
-// (every other reduction: the PCG vector dots, D2, E(t), plain dots) cuts the
-// node index range into blocks of RT*KF consecutive nodes, thread t of block
-// b accumulating the KF consecutive nodes b*RT*KF + t*KF + k, k = 0..KF-1, in
-// order; blocks are combined like the apply order's partials.
-// Interior nodes [1,N-1]^3 are cut into tiles of CX planes (x) x TY rows (y) x
-// TZ columns (z); the boundary nodes are enumerated in increasing node index
-// and cut into blocks of RT*BPT (thread t of block b takes the nodes
-// b*RT*BPT + k*RT + t, k = 0..BPT-1, in order). Each tile thread (ly,lz) accumulates its column
-// over the tile's planes in increasing x; a block's RT values are combined by
-// a 32-lane xor butterfly per warp then an 8-way xor butterfly over warps; the
-// partials (tiles first, then boundary blocks) are combined by RT strided
-// sequential sums followed by the same block tree.
-int g_TY = 8, g_TZ = 32, g_BPT = 8;   // apply layout (tiles + boundary blocks); cx = apply_cx(N)
-int g_KF = 2;                                       // flat layout: consecutive nodes per thread
+// partials) follows the operator's slab tiles, described below.  The FLAT
+// order (every other reduction: the PCG vector dots, D2, E(t), plain dots)
+// cuts the node index range into blocks of RT*KF consecutive nodes, thread t
+// of block b accumulating the KF consecutive nodes b*RT*KF + t*KF + k,
+// k = 0..KF-1, in order; blocks are combined like the apply order's partials.
+//
+// Slab tiles: the node grid is cut into tiles of CX planes (x) x R rows (y) x
+// C columns (z), the last tile of each direction possibly short; tile
+// t = (tx*NRB + rb)*NCB + cb starts at plane tx*CX, row rb*R, column cb*C.  A
+// tile's RT threads own the positions j = l + k*RT (k = 0..SK-1) of a plane of
+// (R+2) x (C+2) positions (one halo row / column on each side), position j at
+// row rb*R - 1 + j/(C+2), column cb*C - 1 + j%(C+2); thread l accumulates the
+// tile's own nodes among its positions, plane by plane in increasing x and
+// positions in increasing k.  A block's RT values are combined by a 32-lane xor
+// butterfly per warp then an 8-way xor butterfly over warps; the tile
+// partials are combined by RT strided sequential sums followed by the same
+// block tree.  (C, R, CX) is a fixed function of N, slab_layout below.
 const int RT = 256;
+const int SK = 4;                 // positions per thread
+const int SPOS = RT * SK;         // positions per tile plane, halo included
+const int SLAB_SLOTS = 296;       // co-resident tiles the layout assumes
+int g_KF = 2;                     // flat layout: consecutive nodes per thread
 
-// planes per apply tile as a function of N (the library's choice: the cx in
-// [8, 64] minimising waves x (cx + 1) for 592 co-resident operator tiles)
-int apply_cx(int N) {
-    const long I = N - 1;
-    if (I <= 0) return 16;
-    const long col = ((I + 8 - 1) / 8) * ((I + 32 - 1) / 32);
-    int best = 16;
+struct SlabLayout { int C, R, CX, NCB, NRB, NXB; long ntiles; };
+
+// The library's tile shape: among C >= min(N+1, 30) with (R+2)(C+2) <= SPOS
+// (R as large as that allows) and CX from the first waves of SLAB_SLOTS tiles,
+// the one minimising waves x (CX+2) x ((R+2)(C+2) + 2(R+1)(C+1)); ties keep the
+// smaller C, then fewer waves.
+SlabLayout slab_layout(int N) {
+    const long NN = N + 1;
+    SlabLayout best{};
     long best_cost = -1;
-    for (int cx = 8; cx <= 64; ++cx) {
-        const long chunks = (I + cx - 1) / cx;
-        const long blocks = col * chunks;
-        const long waves = (blocks + 592 - 1) / 592;
-        const long cost = waves * ((cx < I ? cx : I) + 1);
-        if (best_cost < 0 || cost < best_cost) { best_cost = cost; best = cx; }
+    const long cmin = NN < 30 ? NN : 30;
+    for (long C = cmin; C <= NN; ++C) {
+        const long Cw = C + 2;
+        const long Rmax = SPOS / Cw - 2;
+        if (Rmax < 1) break;
+        const long R = Rmax < NN ? Rmax : NN;
+        const long NCB = (NN + C - 1) / C, NRB = (NN + R - 1) / R, tyz = NCB * NRB;
+        const long work = Cw * (R + 2) + 2 * (C + 1) * (R + 1);
+        const long w0 = (tyz + SLAB_SLOTS - 1) / SLAB_SLOTS;
+        for (long w = w0; w < w0 + 4; ++w) {
+            long nx = w * SLAB_SLOTS / tyz;
+            if (nx < 1) continue;
+            if (nx > NN) nx = NN;
+            const long CX = (NN + nx - 1) / nx;
+            const long NXB = (NN + CX - 1) / CX;
+            const long waves = (tyz * NXB + SLAB_SLOTS - 1) / SLAB_SLOTS;
+            const long cost = waves * (CX + 2) * work;
+            if (best_cost < 0 || cost < best_cost) {
+                best_cost = cost;
+                best.C = (int)C; best.R = (int)R; best.CX = (int)CX;
+                best.NCB = (int)NCB; best.NRB = (int)NRB; best.NXB = (int)NXB;
+                best.ntiles = tyz * NXB;
+            }
+        }
     }
     return best;
 }
-int g_cx_override = 0;   // or_set_layout: fixed cx instead of apply_cx(N)
+SlabLayout g_slab_override{};     // or_set_layout: a fixed tile shape (C > 0) instead of slab_layout(N)
 
 inline double tree256(const double* v) {
     double ws[8];
@@ -303,16 +329,19 @@ struct Oracle {
         }
     }
 
-    // canonical node sum: lower x-plane first, then (ey, ez) order
+    // canonical node sum: from +0.0, the contribution of the element at whose
+    // corner q the node sits, for q = 4, 7, 6, 5, 0, 3, 2, 1 (lower x layer
+    // first, each layer's own-column element first), elements in the domain
     void gather_nodes(double* y) const {
+        static const int order[8] = {4, 7, 6, 5, 0, 3, 2, 1};
         #pragma omp parallel for schedule(static)
         for (long n = 0; n < Nn; ++n) {
             int ix = (int)(n / ((long)NN * NN)), iy = (int)((n / NN) % NN), iz = (int)(n % NN);
             double acc = 0.0;
-            for (int a = 0; a < 2; ++a) for (int b = 0; b < 2; ++b) for (int c = 0; c < 2; ++c) {
-                int ex = ix - 1 + a, ey = iy - 1 + b, ez = iz - 1 + c;
+            for (int s = 0; s < 8; ++s) {
+                const int q = order[s];
+                int ex = ix - ((q >> 2) & 1), ey = iy - ((q >> 1) & 1), ez = iz - (q & 1);
                 if (ex < 0 || ey < 0 || ez < 0 || ex >= N || ey >= N || ez >= N) continue;
-                int q = ((1 - a) << 2) | ((1 - b) << 1) | (1 - c);
                 acc = acc + ye_buf[((size_t)(((long)ex * N + ey) * N + ez)) * 8 + q];
             }
             y[n] = acc;
@@ -332,64 +361,35 @@ struct Oracle {
     }
 
     // ---- canonical reduction ---------------------------------------------------
-    long n_boundary() const { return (long)NN * NN * NN - (long)(N - 1) * (N - 1) * (N - 1); }
-    long bnd_node(long j) const {
-        long P = (long)NN * NN;
-        if (j < P) return j;
-        long jj = j - P;
-        long R = 4L * N;
-        if (jj < (long)(N - 1) * R) {
-            int ix = 1 + (int)(jj / R);
-            long r = jj % R;
-            int iy, iz;
-            if (r < NN) { iy = 0; iz = (int)r; }
-            else if (r < NN + 2L * (N - 1)) { long t = r - NN; iy = 1 + (int)(t / 2); iz = (t & 1) ? N : 0; }
-            else { iy = N; iz = (int)(r - NN - 2L * (N - 1)); }
-            return nid(ix, iy, iz);
-        }
-        jj -= (long)(N - 1) * R;
-        return (long)N * P + jj;
-    }
-
     template <class Term>
     double creduce(Term term) const {
-        std::vector<double> P;
-        const int I = N - 1;
-        const int CXN = g_cx_override ? g_cx_override : apply_cx(N);
-        const int NTX = (I + CXN - 1) / CXN, NTY = (I + g_TY - 1) / g_TY, NTZ = (I + g_TZ - 1) / g_TZ;
-        const int nt = (I > 0) ? NTX * NTY * NTZ : 0;
-        P.resize(nt);
+        SlabLayout L = slab_layout(N);
+        if (g_slab_override.C > 0) {
+            L = g_slab_override;
+            L.NCB = (NN + L.C - 1) / L.C; L.NRB = (NN + L.R - 1) / L.R; L.NXB = (NN + L.CX - 1) / L.CX;
+            L.ntiles = (long)L.NCB * L.NRB * L.NXB;
+        }
+        const int Cw = L.C + 2, Rw = L.R + 2;
+        std::vector<double> P(L.ntiles);
         #pragma omp parallel for schedule(static)
-        for (int t = 0; t < nt; ++t) {
-            int tz = t % NTZ, ty = (t / NTZ) % NTY, tx = t / (NTZ * NTY);
+        for (long t = 0; t < L.ntiles; ++t) {
+            const int cb = (int)(t % L.NCB), rb = (int)((t / L.NCB) % L.NRB), tx = (int)(t / ((long)L.NCB * L.NRB));
+            const int y0 = rb * L.R, z0 = cb * L.C, xa = tx * L.CX, xb = std::min(xa + L.CX, NN) - 1;
             double v[RT];
             for (int l = 0; l < RT; ++l) {
-                int ly = l / g_TZ, lz = l % g_TZ;
                 double acc = 0.0;
-                int iy = 1 + ty * g_TY + ly, iz = 1 + tz * g_TZ + lz;
-                if (ly < g_TY && iy <= I && iz <= I) {
-                    int x0 = 1 + tx * CXN, x1 = std::min(tx * CXN + CXN, I);
-                    for (int ix = x0; ix <= x1; ++ix) acc = term(nid(ix, iy, iz), acc);
-                }
+                for (int ix = xa; ix <= xb; ++ix)
+                    for (int k = 0; k < SK; ++k) {
+                        const int j = l + k * RT;
+                        if (j >= Rw * Cw) continue;
+                        const int lr = j / Cw, lc = j % Cw;
+                        const int iy = y0 - 1 + lr, iz = z0 - 1 + lc;
+                        if (lr < 1 || lr > L.R || lc < 1 || lc > L.C || iy > N || iz > N) continue;
+                        acc = term(nid(ix, iy, iz), acc);
+                    }
                 v[l] = acc;
             }
             P[t] = tree256(v);
-        }
-        long NB = n_boundary();
-        const long RB = (long)RT * g_BPT;
-        long nb = (NB + RB - 1) / RB;
-        for (long b = 0; b < nb; ++b) {
-            double v[RT];
-            for (int l = 0; l < RT; ++l) {
-                double acc = 0.0;
-                for (int k = 0; k < g_BPT; ++k) {
-                    long j = b * RB + (long)k * RT + l;
-                    if (j >= NB) break;
-                    acc = term(bnd_node(j), acc);
-                }
-                v[l] = acc;
-            }
-            P.push_back(tree256(v));
         }
         double v[RT];
         for (int l = 0; l < RT; ++l) {
@@ -612,10 +612,19 @@ struct or_step_out {
     int snap;  // 1 if this step was a snapshot
 };
 
-void or_set_layout(int cx, int ty, int tz, int bpt, int kf) {  // kf: flat nodes per thread
-    g_cx_override = cx; g_TY = ty; g_TZ = tz; g_BPT = bpt; g_KF = kf;
+// apply tile shape (cx planes, ty rows, tz columns; 0 = the per-N shape) and the
+// flat order's nodes per thread kf
+void or_set_layout(int cx, int ty, int tz, int kf) {
+    g_slab_override = SlabLayout{};
+    if (cx > 0 && ty > 0 && tz > 0) { g_slab_override.C = tz; g_slab_override.R = ty; g_slab_override.CX = cx; }
+    g_KF = kf;
 }
-int or_apply_cx(int N) { return apply_cx(N); }
+// the per-N tile shape: out[0..2] = cx, ty (rows), tz (columns); returns the tile count
+long or_slab_layout(int N, int* out3) {
+    const SlabLayout L = slab_layout(N);
+    out3[0] = L.CX; out3[1] = L.R; out3[2] = L.C;
+    return L.ntiles;
+}
 
 int or_set_threads(int n) {
 #ifdef _OPENMP

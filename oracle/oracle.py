@@ -61,9 +61,9 @@ def lib():
         L.or_verify.argtypes = [vp, C.c_int, C.c_int, C.c_double, C.POINTER(C.c_long)]
         L.or_get_vectors.argtypes = [vp, vp, vp, vp, vp, vp]
         L.or_get_matrices.argtypes = [vp, vp, vp, vp]
-        L.or_set_layout.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
-        L.or_apply_cx.restype = C.c_int
-        L.or_apply_cx.argtypes = [C.c_int]
+        L.or_set_layout.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int]
+        L.or_slab_layout.restype = C.c_long
+        L.or_slab_layout.argtypes = [C.c_int, C.POINTER(C.c_int)]
         L.or_set_threads.restype = C.c_int
         L.or_set_threads.argtypes = [C.c_int]
         L.or_initial_condition.argtypes = [vp, dp]
@@ -75,16 +75,19 @@ def _ptr(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
 
 
-def set_layout(cx: int = 0, ty: int = 8, tz: int = 32, bpt: int = 8, kf: int = 2) -> None:
-    """Canonical reduction orders: the apply order's tile (planes cx -- 0 for
-    the library's per-N choice apply_cx(N) --, rows ty, columns tz, boundary
-    nodes per thread bpt) and the flat order's nodes per thread kf.  The
-    defaults are the library's; the block thread count is fixed at 256."""
-    lib().or_set_layout(cx, ty, tz, bpt, kf)
+def set_layout(cx: int = 0, ty: int = 0, tz: int = 0, kf: int = 2) -> None:
+    """Canonical reduction orders: the apply order's slab tile (planes cx, rows
+    ty, columns tz; all 0 for the library's per-N shape slab_layout(N)) and
+    the flat order's nodes per thread kf.  The defaults are the library's; a
+    block has 256 threads of 4 positions each."""
+    lib().or_set_layout(cx, ty, tz, kf)
 
 
-def apply_cx(N: int) -> int:
-    return lib().or_apply_cx(int(N))
+def slab_layout(N: int) -> dict:
+    """The per-N apply tile shape: planes cx, rows ty, columns tz, and the tile count."""
+    out = (C.c_int * 3)()
+    nt = lib().or_slab_layout(int(N), out)
+    return dict(cx=out[0], ty=out[1], tz=out[2], ntiles=int(nt))
 
 
 def set_threads(n: int) -> int:

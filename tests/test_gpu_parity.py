@@ -49,6 +49,31 @@ def test_apply_bitwise(oracle, dev, form, N):
     g.close()
 
 
+@pytest.mark.parametrize("N", [64, 97, 130])
+def test_apply_bitwise_split_tiles(oracle, dev, N):
+    """Grids whose slab tiles split in every direction: halo rows, columns and
+    planes shared between tiles, short last tiles."""
+    lay = oracle.slab_layout(N)
+    assert lay["tz"] < N + 1 and lay["ty"] < N + 1 and lay["cx"] < N + 1
+    o, g = pair(oracle, N, "wht", seed=N)
+    x = random_nodes(N, 200 + N)
+    xd, yd = dev.put(x), dev.zeros(o.Nn)
+    rel = g.apply_ptr(xd.data_ptr(), yd.data_ptr(), dt_eff=o.dt, project=True)
+    y_ref, rel_ref = o.apply(x, dt_eff=o.dt, project=True, d1=True)
+    assert np.array_equal(bits(dev.get(yd)), bits(y_ref))
+    assert np.float64(rel).view(np.uint64) == np.float64(rel_ref).view(np.uint64)
+    g.close()
+
+
+def test_apply_rejects_overlap(oracle, dev):
+    o, g = pair(oracle, 8, "wht")
+    xd = dev.put(random_nodes(8, 1))
+    with pytest.raises(_lib.HeatError) as e:
+        g.apply_ptr(xd.data_ptr(), xd.data_ptr(), project=True)
+    assert e.value.status == 1
+    g.close()
+
+
 @pytest.mark.parametrize("N", SIZES)
 def test_setup_vectors_and_dot(oracle, dev, N):
     o, g = pair(oracle, N, "wht", seed=3 * N)

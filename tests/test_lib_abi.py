@@ -30,13 +30,15 @@ def test_header_symbols_exported():
 
 def test_api_version_and_layout(oracle):
     """The library's canonical reduction orders are the oracle's, for every grid size."""
-    assert _lib.lib().hs_api_version() == 1
+    assert _lib.lib().hs_api_version() == 2
     lay = _lib.layout(128)
-    assert lay["rt"] == 256 and lay["ty"] * lay["tz"] == 256
-    assert (lay["ty"], lay["tz"], lay["bpt"], lay["kf"]) == (8, 32, 8, 2)
+    assert lay["rt"] == 256 and lay["bpt"] == 4 and lay["kf"] == 2
     for N in range(1, 1201):
-        assert _lib.layout(N)["cx"] == oracle.apply_cx(N), N
-        assert 8 <= _lib.layout(N)["cx"] <= 64
+        got, want = _lib.layout(N), oracle.slab_layout(N)
+        assert (got["cx"], got["ty"], got["tz"]) == (want["cx"], want["ty"], want["tz"]), N
+        # a tile plane with its halo fits the CTA's positions; full coverage
+        assert (got["ty"] + 2) * (got["tz"] + 2) <= 256 * 4, N
+        assert got["tz"] >= min(N + 1, 30), N
 
 
 def test_no_oracle_in_library():

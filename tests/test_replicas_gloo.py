@@ -40,7 +40,7 @@ def _rank_main(rank, world, port, out):
 
 def test_replica_aggregation_two_ranks():
     port = _free_port()
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:
         out = m.dict()
         mp.spawn(_rank_main, args=(2, port, out), nprocs=2, join=True)
         res = dict(out)
