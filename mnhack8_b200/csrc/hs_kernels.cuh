@@ -257,13 +257,28 @@ __device__ __forceinline__ void store_partials(double (&v)[NQ], double* partials
 }
 // Final combination of nblk partials per quantity (one CTA of RT threads):
 // RT strided sequential sums, then the canonical tree; valid in thread 0.
+// The strided sums take their partials in batches of FB per quantity: all the
+// batch's loads are issued before the (in-order) adds, so the pass costs a
+// few memory latencies instead of one per partial.
 template <int NQ>
 __device__ __forceinline__ void final_sums(double (&v)[NQ], const double* partials, long long nblk, double (*sh)[8]) {
+    constexpr int FB = 8;
 #pragma unroll
-    for (int q = 0; q < NQ; ++q) {
-        double acc = 0.0;
-        for (long long k = threadIdx.x; k < nblk; k += RT) acc = dadd(acc, __ldcg(partials + q * nblk + k));
-        v[q] = acc;
+    for (int q = 0; q < NQ; ++q) v[q] = 0.0;
+    for (long long k0 = threadIdx.x; k0 < nblk; k0 += (long long)RT * FB) {
+        double t[NQ][FB];
+#pragma unroll
+        for (int q = 0; q < NQ; ++q)
+#pragma unroll
+            for (int u = 0; u < FB; ++u) {
+                const long long k = k0 + (long long)u * RT;
+                t[q][u] = (k < nblk) ? __ldcg(partials + q * nblk + k) : 0.0;
+            }
+#pragma unroll
+        for (int q = 0; q < NQ; ++q)
+#pragma unroll
+            for (int u = 0; u < FB; ++u)
+                if (k0 + (long long)u * RT < nblk) v[q] = dadd(v[q], t[q][u]);
     }
     cta_tree_sum<NQ>(v, sh);
 }
@@ -278,8 +293,7 @@ struct ApplyArgs {
     double* pbuf0;          // LOOP: p double buffer, p_k in pbuf[k & 1]
     double* pbuf1;
     double* y;              // output
-    const double* rhoc;
-    const double* kc;
+    const double2* coef;    // per element (rho*c, k)
     const double* w;        // ABFT weight (w_M or w_A) or null
     const double* F;        // ROLE_RHS source (null: none)
     double dtF;
@@ -330,15 +344,16 @@ __device__ __forceinline__ void slab_march(const ApplyArgs& a, SlabSmem& S, cons
     const unsigned fl = G.fl;
     const int xa = T.xa, xb = T.xb;
 
-    double pc[SK], pn[SK], ra[SK], rb[SK], cr[SK], ck[SK], wv[SK], fv[SK], acc[SK], accn[SK];
+    double pA[SK], pB[SK], aA[SK], aB[SK], ra[SK], rb[SK], cr[SK], ck[SK], wv[SK], fv[SK];
     auto ld_raw = [&](int px) {
         const bool pv = px >= 0 && px <= N;
-        const long long base = (long long)px * plane;
+        const double* sa = src_a + (long long)px * plane;
+        const double* sb = TWO ? src_b + (long long)px * plane : nullptr;
 #pragma unroll
         for (int k = 0; k < SK; ++k) {
             const bool v = pv && sp_valid(fl, k);
-            ra[k] = v ? __ldg(src_a + base + G.noff[k]) : 0.0;
-            if (TWO) rb[k] = v ? __ldg(src_b + base + G.noff[k]) : 0.0;
+            ra[k] = v ? __ldg(sa + G.noff[k]) : 0.0;
+            if (TWO) rb[k] = v ? __ldg(sb + G.noff[k]) : 0.0;
         }
     };
     auto form = [&](int px, double (&p)[SK]) {
@@ -352,12 +367,12 @@ __device__ __forceinline__ void slab_march(const ApplyArgs& a, SlabSmem& S, cons
     };
     auto ld_coef = [&](int ex) {
         const bool ev = ex >= 0 && ex < N;
-        const long long base = (long long)ex * eplane;
+        const double2* ce = a.coef + (long long)ex * eplane;
 #pragma unroll
         for (int k = 0; k < SK; ++k) {
             const bool v = ev && sp_elem(fl, k);
-            cr[k] = v ? __ldg(a.rhoc + base + G.eoff[k]) : 0.0;
-            ck[k] = v ? __ldg(a.kc + base + G.eoff[k]) : 0.0;
+            const double2 c = v ? __ldg(ce + G.eoff[k]) : make_double2(0.0, 0.0);
+            cr[k] = c.x; ck[k] = c.y;
         }
     };
     auto ld_w = [&](int px) {
@@ -371,16 +386,11 @@ __device__ __forceinline__ void slab_march(const ApplyArgs& a, SlabSmem& S, cons
         }
     };
 
-    // plane xa-1, then the inputs of plane xa and the coefficients of layer xa-1
-    ld_raw(xa - 1);
-    form(xa - 1, pc);
-#pragma unroll
-    for (int k = 0; k < SK; ++k) { S.P[(xa - 1) & 1][tid + k * ST] = pc[k]; acc[k] = 0.0; accn[k] = 0.0; }
-    ld_raw(xa);
-    ld_coef(xa - 1);
-
-    for (int ix = xa - 1; ix <= xb; ++ix) {
-        const int cur = ix & 1, nxt = (ix + 1) & 1;
+    // One element layer ix (between planes ix and ix+1).  Plane px lives in
+    // P[(px - xa + 1) & 1] (cur for plane ix); pc / pn hold planes ix / ix+1
+    // of the own column, ac / an the node sums of planes ix / ix+1.
+    auto layer = [&](int ix, int cur, double (&pc)[SK], double (&pn)[SK], double (&ac)[SK], double (&an)[SK]) {
+        const int nxt = cur ^ 1;
         // 1. plane ix+1
         form(ix + 1, pn);
 #pragma unroll
@@ -404,8 +414,8 @@ __device__ __forceinline__ void slab_march(const ApplyArgs& a, SlabSmem& S, cons
                 v[7] = S.P[nxt][j + Cw + 1];
                 elem_apply<FORM>(v, cr[k], ck[k], a.dt_eff, a.ec);
                 if (fi_r && (long long)ix * eplane + G.eoff[k] == fi_elem) v[0] = flipbit(v[0], fi_bit);
-                acc[k] = dadd(acc[k], v[0]);
-                accn[k] = dadd(0.0, v[4]);
+                ac[k] = dadd(ac[k], v[0]);
+                an[k] = dadd(0.0, v[4]);
                 S.Y1[j + 1] = make_double2(v[1], v[5]);
                 S.Y2[j + Cw] = make_double2(v[2], v[6]);
                 S.Y3[j + Cw + 1] = make_double2(v[3], v[7]);
@@ -413,7 +423,7 @@ __device__ __forceinline__ void slab_march(const ApplyArgs& a, SlabSmem& S, cons
         }
         ld_coef(ix + 1 <= xb ? ix + 1 : -1);
         __syncthreads();
-        // 3. tile nodes of plane ix; accumulators of plane ix+1
+        // 3. tile nodes of plane ix; node sums of plane ix+1
         const long long base = (long long)ix * plane;
         const bool xbnd = ix == 0 || ix == N;
 #pragma unroll
@@ -426,7 +436,7 @@ __device__ __forceinline__ void slab_march(const ApplyArgs& a, SlabSmem& S, cons
             if (ix >= xa) {
                 const long long n = base + G.noff[k];
                 const bool bnd = !yzin || xbnd;
-                double y = bnd ? 0.0 : dadd(dadd(dadd(acc[k], y3.x), y2.x), y1.x);
+                double y = bnd ? 0.0 : dadd(dadd(dadd(ac[k], y3.x), y2.x), y1.x);
                 if (fi_ap && n == fi_idx) y = flipbit(y, fi_bit);
                 const double pv = pc[k];
                 if (loop) part[0] = dfma(pv, y, part[0]);
@@ -439,57 +449,63 @@ __device__ __forceinline__ void slab_march(const ApplyArgs& a, SlabSmem& S, cons
                 a.y[n] = y;
                 if (TWO || MODE == 1) pout[n] = pv;
             }
-            acc[k] = yzin ? dadd(dadd(dadd(accn[k], y3.y), y2.y), y1.y) : 0.0;
+            an[k] = yzin ? dadd(dadd(dadd(an[k], y3.y), y2.y), y1.y) : 0.0;
         }
         ld_w(ix + 1);
+    };
+
+    // plane xa-1, then the inputs of plane xa and the coefficients of layer xa-1
+    ld_raw(xa - 1);
+    form(xa - 1, pA);
 #pragma unroll
-        for (int k = 0; k < SK; ++k) pc[k] = pn[k];
+    for (int k = 0; k < SK; ++k) { S.P[0][tid + k * ST] = pA[k]; aA[k] = 0.0; aB[k] = 0.0; }
+    ld_raw(xa);
+    ld_coef(xa - 1);
+    for (int ix = xa - 1; ix <= xb; ++ix) {
+        layer(ix, (ix - xa + 1) & 1, pA, pB, aA, aB);
+#pragma unroll
+        for (int k = 0; k < SK; ++k) { pA[k] = pB[k]; aA[k] = aB[k]; }
     }
 }
 
 // Colored operator: tile blockIdx.x of the slab partition (every node of the
 // grid belongs to exactly one tile; boundary nodes are projected to zero).
-template <int FORM>
+// LOOP: the PCG-loop role (p formed in the kernel); otherwise the roles that
+// apply the operator to a given vector.
+template <int FORM, bool LOOP>
 __global__ void __launch_bounds__(ST, FORM == FORM_WHT ? 2 : 1) k_apply_slab(ApplyArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SlabSmem& S = *reinterpret_cast<SlabSmem*>(smem_raw);
     DevState* st = a.st;
-    const bool loop = a.role == ROLE_LOOP;
-    int iter = 0;
-    double beta = 0.0;
-    const double* src_a = a.x;
-    const double* src_b = nullptr;
-    double* pout = nullptr;
     int fi_p = 0, fi_ap = 0, fi_r = 0, fi_bit = 0;
     long long fi_idx = -1, fi_elem = -1;
-    if (loop) {
+    const bool d1 = a.d1 != 0;
+    double part[MAXQ] = {0.0, 0.0, 0.0, 0.0};
+    const SlabTile T = slab_tile(a.part, blockIdx.x);
+    const SlabPos G = slab_pos(a.part, T, threadIdx.x);
+    if (LOOP) {
         if (st->done) return;
-        iter = st->iter; beta = st->beta;
-        src_a = a.z;
-        src_b = (iter > 0) ? ((iter & 1) ? a.pbuf0 : a.pbuf1) : nullptr;
-        pout = (iter & 1) ? a.pbuf1 : a.pbuf0;
+        const int iter = st->iter;
+        const double beta = st->beta;
+        const double* src_b = (iter > 0) ? ((iter & 1) ? a.pbuf0 : a.pbuf1) : nullptr;
+        double* pout = (iter & 1) ? a.pbuf1 : a.pbuf0;
         if (st->fi_vec && st->fi_iter == iter) {
             fi_idx = st->fi_idx; fi_bit = st->fi_bit;
             fi_p = (st->fi_vec == FI_P); fi_ap = (st->fi_vec == FI_AP);
         }
-    } else if (a.role == ROLE_X0 && st->fi_armR) {
-        fi_r = 1; fi_elem = st->fi_elem; fi_bit = st->fi_bit;
+        if (!src_b)
+            slab_march<FORM, 1>(a, S, T, G, a.z, src_b, beta, pout, true, d1, false, fi_p, fi_ap, 0, fi_bit, fi_idx,
+                                -1, part);
+        else
+            slab_march<FORM, 2>(a, S, T, G, a.z, src_b, beta, pout, true, d1, false, fi_p, fi_ap, 0, fi_bit, fi_idx,
+                                -1, part);
+    } else {
+        if (a.role == ROLE_X0 && st->fi_armR) { fi_r = 1; fi_elem = st->fi_elem; fi_bit = st->fi_bit; }
+        const bool rhs = (a.role == ROLE_RHS) && a.F != nullptr;
+        slab_march<FORM, 0>(a, S, T, G, a.x, nullptr, 0.0, nullptr, false, d1, rhs, 0, 0, fi_r, fi_bit, -1, fi_elem,
+                            part);
+        if (!d1) return;
     }
-    const bool d1 = a.d1 != 0;
-    const bool rhs = (a.role == ROLE_RHS) && a.F != nullptr;
-    double part[MAXQ] = {0.0, 0.0, 0.0, 0.0};
-    const SlabTile T = slab_tile(a.part, blockIdx.x);
-    const SlabPos G = slab_pos(a.part, T, threadIdx.x);
-    if (!loop)
-        slab_march<FORM, 0>(a, S, T, G, src_a, src_b, beta, pout, loop, d1, rhs, fi_p, fi_ap, fi_r, fi_bit, fi_idx,
-                            fi_elem, part);
-    else if (!src_b)
-        slab_march<FORM, 1>(a, S, T, G, src_a, src_b, beta, pout, loop, d1, rhs, fi_p, fi_ap, fi_r, fi_bit, fi_idx,
-                            fi_elem, part);
-    else
-        slab_march<FORM, 2>(a, S, T, G, src_a, src_b, beta, pout, loop, d1, rhs, fi_p, fi_ap, fi_r, fi_bit, fi_idx,
-                            fi_elem, part);
-    if (!loop && !d1) return;
     store_partials<MAXQ>(part, a.partials, a.part.nblk, S.sh);
 }
 

@@ -66,6 +66,7 @@ struct hs_solver {
     cudaStream_t s = nullptr;
 
     DevBuf<double> rhoc, kc, gtab;
+    DevBuf<double2> coef;               // (rho*c, k) per element, the operator kernel's layout
     DevBuf<double> diag, F, wM, wA;
     DevBuf<double> T, b, r, z, p0, p1, Ap;
     DevBuf<double> partials;
@@ -120,22 +121,32 @@ hs_status sync_state_config(hs_solver* h, int max_iter, double tol) {
 int nblocks(const hs_solver* h) { return (int)h->part.nblk; }
 
 // ---- operator launches -------------------------------------------------------------
+template <int FORM>
+bool set_smem_form() {
+    return cudaFuncSetAttribute(k_apply_slab<FORM, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kSlabSmem) == cudaSuccess &&
+           cudaFuncSetAttribute(k_apply_slab<FORM, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kSlabSmem) == cudaSuccess;
+}
 bool set_smem_attributes() {
     static bool done = false, ok = true;
     if (done) return ok;
     done = true;
-    ok = cudaFuncSetAttribute(k_apply_slab<FORM_WHT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSlabSmem) == cudaSuccess &&
-         cudaFuncSetAttribute(k_apply_slab<FORM_FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSlabSmem) == cudaSuccess &&
-         cudaFuncSetAttribute(k_apply_slab<FORM_GAUSS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSlabSmem) == cudaSuccess;
+    ok = set_smem_form<FORM_WHT>() && set_smem_form<FORM_FAST>() && set_smem_form<FORM_GAUSS>();
     return ok;
 }
 
-void launch_colored(hs_solver* h, const ApplyArgs& a) {
+template <int FORM>
+void launch_slab(hs_solver* h, const ApplyArgs& a) {
     const int g = (int)h->part.ntiles;
+    if (a.role == ROLE_LOOP) k_apply_slab<FORM, true><<<g, ST, kSlabSmem, h->s>>>(a);
+    else k_apply_slab<FORM, false><<<g, ST, kSlabSmem, h->s>>>(a);
+}
+void launch_colored(hs_solver* h, const ApplyArgs& a) {
     switch (h->opt.kernel) {
-        case HS_KERNEL_WHT: k_apply_slab<FORM_WHT><<<g, ST, kSlabSmem, h->s>>>(a); break;
-        case HS_KERNEL_GAUSS: k_apply_slab<FORM_GAUSS><<<g, ST, kSlabSmem, h->s>>>(a); break;
-        default: k_apply_slab<FORM_FAST><<<g, ST, kSlabSmem, h->s>>>(a); break;
+        case HS_KERNEL_WHT: launch_slab<FORM_WHT>(h, a); break;
+        case HS_KERNEL_GAUSS: launch_slab<FORM_GAUSS>(h, a); break;
+        default: launch_slab<FORM_FAST>(h, a); break;
     }
 }
 void launch_nodes(hs_solver* h, const GenArgs& a) {
@@ -165,7 +176,7 @@ void apply_projected(hs_solver* h, int role, const double* x, double* y, double 
         a.part = h->part;
         a.N = h->N; a.role = role; a.dt_eff = dt_eff;
         a.x = x; a.z = h->z.p; a.pbuf0 = h->p0.p; a.pbuf1 = h->p1.p;
-        a.y = y; a.rhoc = h->rhoc.p; a.kc = h->kc.p; a.w = w; a.F = F; a.dtF = dtF;
+        a.y = y; a.coef = h->coef.p; a.w = w; a.F = F; a.dtF = dtF;
         a.d1 = d1 ? 1 : 0;
         a.partials = h->partials.p; a.st = h->st.p; a.ec = h->ec;
         launch_colored(h, a);
@@ -403,7 +414,7 @@ hs_status hs_create(const hs_options* opt, const double* k_host, const double* r
 
     HS_CUDA(cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking));
     const size_t Nn = (size_t)h->Nn, Ne = (size_t)h->Ne;
-    HS_CUDA(h->rhoc.alloc(Ne)); HS_CUDA(h->kc.alloc(Ne)); HS_CUDA(h->gtab.alloc(256));
+    HS_CUDA(h->rhoc.alloc(Ne)); HS_CUDA(h->kc.alloc(Ne)); HS_CUDA(h->gtab.alloc(256)); HS_CUDA(h->coef.alloc(Ne));
     HS_CUDA(h->diag.alloc(Nn)); HS_CUDA(h->F.alloc(Nn));
     HS_CUDA(h->T.alloc(Nn)); HS_CUDA(h->b.alloc(Nn)); HS_CUDA(h->r.alloc(Nn)); HS_CUDA(h->z.alloc(Nn));
     HS_CUDA(h->p0.alloc(Nn)); HS_CUDA(h->p1.alloc(Nn)); HS_CUDA(h->Ap.alloc(Nn));
@@ -415,6 +426,12 @@ hs_status hs_create(const hs_options* opt, const double* k_host, const double* r
         HS_CUDA(cudaMemsetAsync(v->p, 0, Nn * sizeof(double), h->s));
     HS_CUDA(cudaMemcpyAsync(h->rhoc.p, rhoc_host, Ne * 8, cudaMemcpyHostToDevice, h->s));
     HS_CUDA(cudaMemcpyAsync(h->kc.p, k_host, Ne * 8, cudaMemcpyHostToDevice, h->s));
+    {
+        std::vector<double2> ce((size_t)Ne);
+        for (long long e = 0; e < Ne; ++e) ce[e] = make_double2(rhoc_host[e], k_host[e]);
+        HS_CUDA(cudaMemcpyAsync(h->coef.p, ce.data(), Ne * 16, cudaMemcpyHostToDevice, h->s));
+        HS_CUDA(cudaStreamSynchronize(h->s));
+    }
     HS_CUDA(cudaMemcpyAsync(h->gtab.p, h->mats.gtab, 256 * 8, cudaMemcpyHostToDevice, h->s));
     h->ec.gtab = h->gtab.p;
 
