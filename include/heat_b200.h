@@ -197,6 +197,32 @@ typedef struct hs_twin_summary {
 hs_status hs_classify(const hs_step_record* A, const hs_step_record* B, const hs_step_record* F, int n_steps,
                       int fi_level, int F_nonfinite, double dt, double thr_user, int detect, hs_twin_summary* out);
 
+/* One flip of a fault-injection campaign and the twin-run outcome. */
+typedef struct hs_flip_record {
+    int step;                 /* time step of the flip */
+    int iter;                 /* PCG iteration of the flip */
+    int level;                /* HS_FI_P (p after formation), HS_FI_RV (r after its update), HS_FI_AP (Ap) */
+    int bit;                  /* 0..63 */
+    long long idx;            /* vector entry, 0..(N+1)^3-1 */
+    int nonfinite;            /* the faulted run produced a non-finite field */
+    int iters_total_delta;    /* faulted minus clean CG iterations over the trajectory */
+    hs_twin_summary summary;  /* hs_classify(clean, clean twin, faulted) */
+} hs_flip_record;
+
+/* Seeded single-bit-flip campaign over one trajectory.  No counterpart in the
+ * reference, which runs one twin-run process per flip (het.cu:1506-1620).
+ * Runs the clean trajectory (kept as the reference, with its field at the
+ * start of every step), its clean twin, then n_flips faulted trajectories,
+ * each resumed at its flip step from the kept clean field (colored scatter
+ * only).  Flip sites come from std::mt19937_64(seed), each draw the
+ * generator's next output modulo its range, in this order: a global CG
+ * iteration over the clean run's total (mapped to step and iteration), a
+ * vector among the levels in vec_mask (bit 0 p, bit 1 r, bit 2 Ap), a node
+ * entry, a bit in 0..63.  clean_out (nullable): the clean run's n_steps
+ * records.  Device memory: n_steps extra fields. */
+hs_status hs_campaign(hs_solver* s, int n_steps, int snap_every, int n_flips, unsigned long long seed, int vec_mask,
+                      hs_step_record* clean_out, hs_flip_record* out);
+
 /* x.y over the (N+1)^3 nodes of an N-element grid without allocating any
  * device memory.  No counterpart in the reference.  For callers that cannot
  * call cudaMalloc (a host application that owns the device-memory budget, a

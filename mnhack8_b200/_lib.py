@@ -25,7 +25,7 @@ EXPORTS = [
     "hs_destroy", "hs_num_nodes", "hs_field_stats", "hs_apply", "hs_precond", "hs_build_rhs", "hs_dot", "hs_pcg",
     "hs_arm_fi", "hs_run_case", "hs_verify", "hs_solve_host", "hs_diag_cg", "hs_set_dump", "hs_set_case_tag",
     "hs_target_on_boundary", "hs_classify", "hs_cli_main", "hs_advance", "hs_set_field", "hs_get_field",
-    "hs_time_kernel", "hs_dot_noalloc",
+    "hs_time_kernel", "hs_dot_noalloc", "hs_campaign",
 ]
 
 
@@ -59,6 +59,11 @@ class TwinSummary(C.Structure):
                 ("d3_first", C.c_int), ("pad", C.c_int), ("d1_max", C.c_double), ("d2_max", C.c_double),
                 ("d1_max_A", C.c_double), ("d2_max_A", C.c_double), ("cls", C.c_char * 16),
                 ("detected_by", C.c_char * 16)]
+
+
+class FlipRecord(C.Structure):
+    _fields_ = [("step", C.c_int), ("iter", C.c_int), ("level", C.c_int), ("bit", C.c_int), ("idx", C.c_longlong),
+                ("nonfinite", C.c_int), ("iters_total_delta", C.c_int), ("summary", TwinSummary)]
 
 
 _lib = None
@@ -132,6 +137,8 @@ def lib():
     L.hs_time_kernel.argtypes = [vp, i, i, pd]
     L.hs_dot_noalloc.restype = i
     L.hs_dot_noalloc.argtypes = [i, vp, vp, vp]
+    L.hs_campaign.restype = i
+    L.hs_campaign.argtypes = [vp, i, i, i, C.c_ulonglong, i, C.POINTER(StepRecord), C.POINTER(FlipRecord)]
     L.hs_cli_main.restype = i
     L.hs_cli_main.argtypes = [i, C.POINTER(C.c_char_p)]
     _lib = L
@@ -249,6 +256,25 @@ class Solver:
         steps = [dict(cg_iters=r.cg_iters, snap=r.snap, d1=r.d1, d2=r.d2, tmin=r.tmin, tmax=r.tmax, E=r.E,
                       spread=r.spread, solve_ms=r.solve_ms) for r in recs[:n_steps]]
         return dict(T=T, steps=steps, nonfinite=nf.value, records=recs)
+
+    def campaign(self, n_steps, snap_every, n_flips, seed, vectors=("P", "RV", "AP")):
+        """Seeded single-bit-flip campaign (hs_campaign): the clean run's step
+        records and one dict per flip (site and twin-run summary)."""
+        mask = sum({"P": 1, "RV": 2, "AP": 4}[v] for v in vectors)
+        clean = (StepRecord * max(n_steps, 1))()
+        flips = (FlipRecord * max(n_flips, 1))()
+        check(lib().hs_campaign(self._h, int(n_steps), int(snap_every), int(n_flips), C.c_ulonglong(seed), mask,
+                                clean, flips))
+        steps = [dict(cg_iters=r.cg_iters, snap=r.snap, d1=r.d1, d2=r.d2, tmin=r.tmin, tmax=r.tmax, E=r.E,
+                      spread=r.spread, solve_ms=r.solve_ms) for r in clean[:n_steps]]
+        out = []
+        for r in flips[:n_flips]:
+            sm = r.summary
+            summ = {name: (getattr(sm, name).decode() if name in ("cls", "detected_by") else getattr(sm, name))
+                    for name, _ in TwinSummary._fields_ if name != "pad"}
+            out.append(dict(step=r.step, iter=r.iter, level=r.level, bit=r.bit, idx=r.idx, nonfinite=r.nonfinite,
+                            iters_total_delta=r.iters_total_delta, summary=summ))
+        return steps, out
 
     def verify(self, n_steps):
         rel, ms = C.c_double(), C.c_double()

@@ -618,6 +618,16 @@ hs_status enqueue_step(hs_solver* h, const hs_fi_spec* fi, int step, int reproje
 
 }  // namespace
 
+// where a trajectory starts (run_case_impl)
+struct RunFrom {
+    int s0 = 0;                            // first step computed
+    const double* T_start = nullptr;       // device field at the start of step s0 (s0 > 0)
+    double* const* keep_states = nullptr;  // optional: field at the start of every step
+};
+hs_status run_case_impl(hs_solver* h, int n_steps, int snap_every, const hs_fi_spec* fi, int reproject,
+                        int keep_reference, hs_step_record* out, double* T_final_host, int* nonfinite,
+                        const RunFrom& from);
+
 extern "C" {
 
 hs_status hs_pcg(hs_solver* s, const double* b, double* x, int max_iter, double tol, int* iters) {
@@ -651,19 +661,36 @@ hs_status hs_pcg(hs_solver* s, const double* b, double* x, int max_iter, double 
 
 hs_status hs_run_case(hs_solver* h, int n_steps, int snap_every, const hs_fi_spec* fi, int reproject,
                       int keep_reference, hs_step_record* out, double* T_final_host, int* nonfinite) {
+    return run_case_impl(h, n_steps, snap_every, fi, reproject, keep_reference, out, T_final_host, nonfinite,
+                         RunFrom{});
+}
+
+}  // extern "C"
+
+// One trajectory (run_case, het.cu:1107-1259).  from.s0 > 0 resumes at step
+// s0 from the field from.T_start (records of earlier steps are left to the
+// caller); from.keep_states, if set, receives the field at the start of every
+// step (n_steps device buffers of (N+1)^3 doubles).
+hs_status run_case_impl(hs_solver* h, int n_steps, int snap_every, const hs_fi_spec* fi, int reproject,
+                        int keep_reference, hs_step_record* out, double* T_final_host, int* nonfinite,
+                        const RunFrom& from) {
     if (!h || n_steps < 0 || !out) { set_error("bad arguments"); return HS_ERR_ARG; }
+    if (from.s0 < 0 || from.s0 > n_steps || (from.s0 > 0 && (!from.T_start || keep_reference))) {
+        set_error("bad resume step");
+        return HS_ERR_ARG;
+    }
     hs_status st = validate_fi(h, fi);
     if (st != HS_OK) return st;
-    if (!keep_reference && (int)h->ref_snaps.size() == 0 && n_steps > 0) {
-        // no reference: E is not evaluated
-    }
     st = sync_state_config(h, h->opt.max_iter, h->opt.rtol);
     if (st != HS_OK) return st;
     st = build_graph(h, 0);
     if (st != HS_OK) return st;
     const long long Nn = h->Nn;
-    // initial condition (het.cu:1115-1116)
-    if (h->opt.ic_mode == 1) {
+    const int s0 = from.s0;
+    // initial condition (het.cu:1115-1116), or the resumed field
+    if (s0 > 0) {
+        HS_CUDA(cudaMemcpyAsync(h->T.p, from.T_start, Nn * 8, cudaMemcpyDeviceToDevice, h->s));
+    } else if (h->opt.ic_mode == 1) {
         std::vector<double> T0(Nn);
         gaussian_ic(h->N, h->opt.ic_sigma, T0.data());
         HS_CUDA(cudaMemcpyAsync(h->T.p, T0.data(), Nn * 8, cudaMemcpyHostToDevice, h->s));
@@ -695,8 +722,12 @@ hs_status hs_run_case(hs_solver* h, int n_steps, int snap_every, const hs_fi_spe
     std::vector<cudaEvent_t> ev(2 * (size_t)n_steps);
     for (auto& e : ev) HS_CUDA(cudaEventCreate(&e));
     int si = 0;
-    for (int step = 0; step < n_steps; ++step) {
+    for (int step = 0; step < s0; ++step)
+        if ((snap_every > 0 && step % snap_every == 0) || step == n_steps - 1) ++si;
+    for (int step = s0; step < n_steps; ++step) {
         double* rec = d_rec.p + (size_t)step * 8;
+        if (from.keep_states)
+            HS_CUDA(cudaMemcpyAsync(from.keep_states[step], h->T.p, Nn * 8, cudaMemcpyDeviceToDevice, h->s));
         st = enqueue_step(h, fi, step, reproject, d_it.p + step, rec + 0, ev[2 * step], ev[2 * step + 1]);
         if (st != HS_OK) return st;
         if (h->opt.detect) {
@@ -742,7 +773,7 @@ hs_status hs_run_case(hs_solver* h, int n_steps, int snap_every, const hs_fi_spe
     int nf = 0;
     si = 0;
     if (keep_reference) { h->ref_tmin.assign(n_steps, 0.0); h->ref_tmax.assign(n_steps, 0.0); }
-    for (int step = 0; step < n_steps; ++step) {
+    for (int step = s0; step < n_steps; ++step) {
         hs_step_record& o = out[step];
         const double* rr = &rec[(size_t)step * 8];
         o.cg_iters = it[step];
@@ -765,6 +796,8 @@ hs_status hs_run_case(hs_solver* h, int n_steps, int snap_every, const hs_fi_spe
     if (T_final_host) HS_CUDA(cudaMemcpy(T_final_host, h->T.p, Nn * 8, cudaMemcpyDeviceToHost));
     return HS_OK;
 }
+
+extern "C" {
 
 hs_status hs_verify(hs_solver* h, int n_steps, double* rel_err, long long* total_iters, double* ms) {
     if (!h) return HS_ERR_ARG;
@@ -1031,3 +1064,5 @@ hs_status hs_time_kernel(hs_solver* h, int which, int reps, double* ms_per_launc
 
 // the allocation-free dot product shares this translation unit's kernels
 #include "hs_noalloc.cu"
+// the fault-injection campaign resumes trajectories through run_case_impl
+#include "hs_campaign.cu"
