@@ -223,6 +223,47 @@ typedef struct hs_flip_record {
 hs_status hs_campaign(hs_solver* s, int n_steps, int snap_every, int n_flips, unsigned long long seed, int vec_mask,
                       hs_step_record* clean_out, hs_flip_record* out);
 
+/* ---- batched mixed-precision solves (no counterpart in the reference) ----
+ * Many independent solves live in one handle and advance together, one
+ * implicit-Euler step of every instance per hs_batch_step (one CUDA-graph
+ * launch).  Each step solves (M + dt K) T = M T_old by defect correction:
+ * FP64 residual r = b - A T with the ABFT checksum, an FP32 Jacobi-PCG solve
+ * of A d = r to inner_tol (FP32 operator and preconditioner, FP64 dot
+ * products), T += d in FP64, until ||b - A T|| / ||b|| < rtol (the true
+ * residual) or max_outer corrections.  Element form wht, deterministic
+ * scatter, Dirichlet T = 0, no source.  Instances can be added and removed
+ * between steps (continuous batching). */
+typedef struct hs_batch hs_batch;
+typedef struct hs_batch_options {
+    double rtol;          /* outer tolerance on ||b - A T|| / ||b||, e.g. 1e-8 */
+    double inner_tol;     /* FP32 inner PCG relative tolerance, e.g. 1e-4 */
+    int max_outer;        /* corrections per step */
+    int max_inner;        /* inner PCG iterations per correction */
+    int detect;           /* ABFT checksum on every operator apply */
+    int tile_split;       /* operator tiles span ceil((N+1) / tile_split) planes */
+    int device;
+    int pad;
+} hs_batch_options;
+typedef struct hs_batch_inst_info {
+    int N, steps_done, steps_left, pad;
+    long long inner_iters, outer_iters, applies32, applies64, tiles;
+    double rel_residual;  /* last true relative residual */
+    double d1_max64;      /* largest D1 of the FP64 applies */
+    double d1_max32;      /* largest D1 of the FP32 applies (their noise floor when clean) */
+} hs_batch_inst_info;
+void      hs_batch_default_options(hs_batch_options* o);
+hs_status hs_batch_create(const hs_batch_options* opt, hs_batch** out);
+void      hs_batch_destroy(hs_batch* b);
+/* k, rhoc: N^3 host arrays; T0: (N+1)^3 host field or null (zero); the
+ * instance takes n_steps steps.  Sets *slot. */
+hs_status hs_batch_add(hs_batch* b, int N, double dt, const double* k, const double* rhoc, const double* T0,
+                       int n_steps, int* slot);
+hs_status hs_batch_remove(hs_batch* b, int slot);
+/* one step of every instance with steps left; device time of the launch */
+hs_status hs_batch_step(hs_batch* b, int* n_active, double* device_ms);
+hs_status hs_batch_info(hs_batch* b, int slot, hs_batch_inst_info* out);
+hs_status hs_batch_get_field(hs_batch* b, int slot, double* T_host);
+
 /* x.y over the (N+1)^3 nodes of an N-element grid without allocating any
  * device memory.  No counterpart in the reference.  For callers that cannot
  * call cudaMalloc (a host application that owns the device-memory budget, a

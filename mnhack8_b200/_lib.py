@@ -25,7 +25,8 @@ EXPORTS = [
     "hs_destroy", "hs_num_nodes", "hs_field_stats", "hs_apply", "hs_precond", "hs_build_rhs", "hs_dot", "hs_pcg",
     "hs_arm_fi", "hs_run_case", "hs_verify", "hs_solve_host", "hs_diag_cg", "hs_set_dump", "hs_set_case_tag",
     "hs_target_on_boundary", "hs_classify", "hs_cli_main", "hs_advance", "hs_set_field", "hs_get_field",
-    "hs_time_kernel", "hs_dot_noalloc", "hs_campaign",
+    "hs_time_kernel", "hs_dot_noalloc", "hs_campaign", "hs_batch_default_options", "hs_batch_create",
+    "hs_batch_destroy", "hs_batch_add", "hs_batch_remove", "hs_batch_step", "hs_batch_info", "hs_batch_get_field",
 ]
 
 
@@ -64,6 +65,18 @@ class TwinSummary(C.Structure):
 class FlipRecord(C.Structure):
     _fields_ = [("step", C.c_int), ("iter", C.c_int), ("level", C.c_int), ("bit", C.c_int), ("idx", C.c_longlong),
                 ("nonfinite", C.c_int), ("iters_total_delta", C.c_int), ("summary", TwinSummary)]
+
+
+class BatchOptions(C.Structure):
+    _fields_ = [("rtol", C.c_double), ("inner_tol", C.c_double), ("max_outer", C.c_int), ("max_inner", C.c_int),
+                ("detect", C.c_int), ("tile_split", C.c_int), ("device", C.c_int), ("pad", C.c_int)]
+
+
+class BatchInstInfo(C.Structure):
+    _fields_ = [("N", C.c_int), ("steps_done", C.c_int), ("steps_left", C.c_int), ("pad", C.c_int),
+                ("inner_iters", C.c_longlong), ("outer_iters", C.c_longlong), ("applies32", C.c_longlong),
+                ("applies64", C.c_longlong), ("tiles", C.c_longlong), ("rel_residual", C.c_double),
+                ("d1_max64", C.c_double), ("d1_max32", C.c_double)]
 
 
 _lib = None
@@ -137,6 +150,22 @@ def lib():
     L.hs_time_kernel.argtypes = [vp, i, i, pd]
     L.hs_dot_noalloc.restype = i
     L.hs_dot_noalloc.argtypes = [i, vp, vp, vp]
+    L.hs_batch_default_options.restype = None
+    L.hs_batch_default_options.argtypes = [C.POINTER(BatchOptions)]
+    L.hs_batch_create.restype = i
+    L.hs_batch_create.argtypes = [C.POINTER(BatchOptions), C.POINTER(vp)]
+    L.hs_batch_destroy.restype = None
+    L.hs_batch_destroy.argtypes = [vp]
+    L.hs_batch_add.restype = i
+    L.hs_batch_add.argtypes = [vp, i, C.c_double, vp, vp, vp, i, C.POINTER(i)]
+    L.hs_batch_remove.restype = i
+    L.hs_batch_remove.argtypes = [vp, i]
+    L.hs_batch_step.restype = i
+    L.hs_batch_step.argtypes = [vp, C.POINTER(i), pd]
+    L.hs_batch_info.restype = i
+    L.hs_batch_info.argtypes = [vp, i, C.POINTER(BatchInstInfo)]
+    L.hs_batch_get_field.restype = i
+    L.hs_batch_get_field.argtypes = [vp, i, vp]
     L.hs_campaign.restype = i
     L.hs_campaign.argtypes = [vp, i, i, i, C.c_ulonglong, i, C.POINTER(StepRecord), C.POINTER(FlipRecord)]
     L.hs_cli_main.restype = i
@@ -350,6 +379,61 @@ def classify(A, B, F, fi_level, dt, thr_user=1e-13, detect=False, F_nonfinite=0)
                             int(detect), C.byref(out)))
     return {name: (getattr(out, name).decode() if name in ("cls", "detected_by") else getattr(out, name))
             for name, _ in TwinSummary._fields_ if name != "pad"}
+
+
+class Batch:
+    """Batched mixed-precision solves (hs_batch_*): instances added to slots
+    advance one implicit-Euler step per step() call, all in one graph launch."""
+
+    def __init__(self, rtol=1e-8, inner_tol=1e-4, max_outer=10, max_inner=500, detect=True, tile_split=1,
+                 device=0):
+        o = BatchOptions()
+        lib().hs_batch_default_options(C.byref(o))
+        o.rtol, o.inner_tol, o.max_outer, o.max_inner = rtol, inner_tol, max_outer, max_inner
+        o.detect, o.tile_split, o.device = int(detect), int(tile_split), int(device)
+        self._h = C.c_void_p()
+        check(lib().hs_batch_create(C.byref(o), C.byref(self._h)))
+        self.Nn = {}
+
+    def add(self, N, dt, k, rhoc, T0=None, steps=1):
+        k, rhoc = _host(k), _host(rhoc)
+        T0 = None if T0 is None else _host(T0)
+        slot = C.c_int(-1)
+        check(lib().hs_batch_add(self._h, int(N), float(dt), k.ctypes.data, rhoc.ctypes.data,
+                                 T0.ctypes.data if T0 is not None else None, int(steps), C.byref(slot)))
+        self.Nn[slot.value] = (N + 1) ** 3
+        return slot.value
+
+    def remove(self, slot):
+        check(lib().hs_batch_remove(self._h, int(slot)))
+        self.Nn.pop(slot, None)
+
+    def step(self):
+        """One step of every instance with steps left: (instances stepped, device ms)."""
+        n, ms = C.c_int(0), C.c_double(0.0)
+        check(lib().hs_batch_step(self._h, C.byref(n), C.byref(ms)))
+        return n.value, ms.value
+
+    def info(self, slot):
+        r = BatchInstInfo()
+        check(lib().hs_batch_info(self._h, int(slot), C.byref(r)))
+        return {name: getattr(r, name) for name, _ in BatchInstInfo._fields_ if name != "pad"}
+
+    def field(self, slot):
+        T = np.empty(self.Nn[slot])
+        check(lib().hs_batch_get_field(self._h, int(slot), T.ctypes.data))
+        return T
+
+    def close(self):
+        if self._h:
+            lib().hs_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def dot_noalloc(N, x_dev, y_dev, out_dev):

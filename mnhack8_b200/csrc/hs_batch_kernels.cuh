@@ -1,0 +1,520 @@
+// hs_batch_kernels.cuh -- kernels of the batched mixed-precision solver
+// (hs_batch.cu).  Many independent transient-heat solves advance together:
+// every launch covers the slab tiles (operator) or flat blocks (vector work)
+// of all instances, and a block finds its instance through a map.  Each
+// implicit-Euler step solves (M + dt K) T = M T_old by defect correction:
+// FP64 residual r = b - A T (the slab operator in FP64, ABFT checked),
+// an FP32 Jacobi-PCG solve of A d = r to a loose relative tolerance (FP32
+// operator and preconditioner, FP64 dot products of the FP32 values), and
+// T += d in FP64, until ||b - A T|| / ||b|| < rtol.
+#pragma once
+#include "hs_kernels.cuh"
+
+namespace hs {
+
+// per-instance scalars, device resident
+struct BState {
+    // inner FP32 PCG
+    double rho, alpha, beta, bn_in;
+    int iter, done, broken, pad0;
+    // outer defect correction
+    double bn64, rel64, d1_last, d1_max64, d1_max32;
+    double norm_wA, norm_wM;
+    int outer, odone, pad1, pad2;
+    // counters over the run
+    long long inner_total, outer_total, applies32, applies64;
+};
+
+// instance descriptor (device array, rewritten by the host between rounds)
+struct BInst {
+    Part part;                 // slab tiles and flat blocks of this instance
+    long long tile0, flat0;    // first global tile / flat block
+    double dt;
+    double cm[4], ck[4];       // wht eigen-constants / 8 of this grid
+    float cmf[4], ckf[4];
+    int active, pad;
+    double* T;                 // solution (updated in place)
+    double* b;                 // right-hand side M T_old
+    double* y64;               // FP64 operator output
+    double* r64;               // FP64 residual
+    const double2* coef64;     // (rho*c, k) per element
+    const float2* coef32;
+    const double* wA;          // ABFT weights A 1_int, M 1_int (FP64)
+    const double* wM;
+    const float* dinv32;       // 1 / diag, FP32
+    float* r32;
+    float* z32;
+    float* p32a;
+    float* p32b;
+    float* Ap32;
+    float* d32;                // correction
+    BState* st;
+};
+
+struct BatchArgs {
+    const BInst* inst;
+    const int* tile2inst;      // global tile -> instance slot (-1: none)
+    const int* flat2inst;      // global flat block -> instance slot
+    int n_inst, pad;
+    long long ntiles, nflat;   // capacity of the grids
+    double* pa;                // apply partials: [q * ntiles + tile]
+    double* pf;                // flat partials:  [q * nflat + block]
+    double rtol, inner_tol;
+    int max_outer, max_inner;
+    int detect, pad2;
+};
+
+template <typename V> struct VTraits;
+template <> struct VTraits<float> {
+    using V2 = float2;
+    __device__ static float add(float a, float b) { return __fadd_rn(a, b); }
+    __device__ static float sub(float a, float b) { return __fsub_rn(a, b); }
+    __device__ static float mul(float a, float b) { return __fmul_rn(a, b); }
+    __device__ static float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+};
+template <> struct VTraits<double> {
+    using V2 = double2;
+    __device__ static double add(double a, double b) { return __dadd_rn(a, b); }
+    __device__ static double sub(double a, double b) { return __dsub_rn(a, b); }
+    __device__ static double mul(double a, double b) { return __dmul_rn(a, b); }
+    __device__ static double fma(double a, double b, double c) { return __fma_rn(a, b, c); }
+};
+
+// the Walsh-Hadamard element operator in precision V (same structure as elem_wht)
+template <typename V>
+__device__ __forceinline__ void elem_wht_v(V* v, V rhoc, V dk, const V* cm, const V* ck) {
+    using T = VTraits<V>;
+#pragma unroll
+    for (int bit = 1; bit <= 4; bit <<= 1)
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+            if (!(q & bit)) { const V u = v[q], w = v[q | bit]; v[q] = T::add(u, w); v[q | bit] = T::sub(u, w); }
+    const V l0 = T::mul(rhoc, cm[0]);
+    const V l1 = T::fma(dk, ck[1], T::mul(rhoc, cm[1]));
+    const V l2 = T::fma(dk, ck[2], T::mul(rhoc, cm[2]));
+    const V l3 = T::fma(dk, ck[3], T::mul(rhoc, cm[3]));
+    v[0] = T::mul(v[0], l0);
+    v[1] = T::mul(v[1], l1); v[2] = T::mul(v[2], l1); v[4] = T::mul(v[4], l1);
+    v[3] = T::mul(v[3], l2); v[5] = T::mul(v[5], l2); v[6] = T::mul(v[6], l2);
+    v[7] = T::mul(v[7], l3);
+#pragma unroll
+    for (int bit = 1; bit <= 4; bit <<= 1)
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+            if (!(q & bit)) { const V u = v[q], w = v[q | bit]; v[q] = T::add(u, w); v[q | bit] = T::sub(u, w); }
+}
+
+template <typename V>
+struct __align__(16) BSlabSmem {
+    V P[2][SPOS];
+    typename VTraits<V>::V2 Y1[SPOS], Y2[SPOS], Y3[SPOS];
+    double sh[MAXQ][8];
+};
+
+// Batched slab operator.  KIND 0: y64 = A T (FP64, residual); 1: b = M T
+// (FP64, right-hand side); 2: inner FP32 loop, p = z (+ beta p), Ap = A p.
+// Partials per tile: p.Ap (KIND 2), and D1: 1_int.y, w.x, x.x.
+enum BKind { BK_RESID = 0, BK_RHS = 1, BK_LOOP = 2 };
+
+template <typename V, int KIND>
+__global__ void __launch_bounds__(ST, 2) kb_apply(BatchArgs B) {
+    using T2 = typename VTraits<V>::V2;
+    using VT = VTraits<V>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    BSlabSmem<V>& S = *reinterpret_cast<BSlabSmem<V>*>(smem_raw);
+    const long long t = blockIdx.x;
+    if (t >= B.ntiles) return;
+    const int slot = B.tile2inst[t];
+    if (slot < 0) return;
+    const BInst& I = B.inst[slot];
+    if (!I.active) return;
+    BState* st = I.st;
+    const bool loop = KIND == BK_LOOP;
+    if constexpr (KIND == BK_LOOP) {
+        if (st->odone || st->done) return;
+    } else if constexpr (KIND == BK_RESID) {
+        if (st->odone) return;
+    }
+    const Part& P = I.part;
+    const int N = P.N, Cw = P.Cw;
+    const long long plane = (long long)P.NN * P.NN, eplane = (long long)N * N;
+    const SlabTile Tt = slab_tile(P, t - I.tile0);
+    const SlabPos G = slab_pos(P, Tt, threadIdx.x);
+    const unsigned fl = G.fl;
+    const int tid = threadIdx.x, xa = Tt.xa, xb = Tt.xb;
+    const V dtv = (V)((KIND == BK_RHS) ? 0.0 : I.dt);
+    V cm[4], ck[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        cm[j] = (sizeof(V) == 4) ? (V)I.cmf[j] : (V)I.cm[j];
+        ck[j] = (sizeof(V) == 4) ? (V)I.ckf[j] : (V)I.ck[j];
+    }
+    // inputs
+    const int iter = loop ? st->iter : 0;
+    const double betad = loop ? st->beta : 0.0;
+    const V beta = (V)betad;
+    const V* src_a;
+    const V* src_b = nullptr;
+    V* pout = nullptr;
+    V* yout;
+    if constexpr (KIND == BK_LOOP) {
+        src_a = reinterpret_cast<const V*>(I.z32);
+        src_b = (iter > 0) ? reinterpret_cast<const V*>((iter & 1) ? I.p32a : I.p32b) : nullptr;
+        pout = reinterpret_cast<V*>((iter & 1) ? I.p32b : I.p32a);
+        yout = reinterpret_cast<V*>(I.Ap32);
+    } else {
+        src_a = reinterpret_cast<const V*>(I.T);
+        yout = reinterpret_cast<V*>(KIND == BK_RHS ? I.b : I.y64);
+    }
+    const bool two = src_b != nullptr;
+    const double* w = (KIND == BK_RHS) ? I.wM : I.wA;
+    const bool d1 = B.detect != 0;
+    double part[MAXQ] = {0.0, 0.0, 0.0, 0.0};
+
+    V pA[SK], pB[SK], aA[SK], aB[SK], ra[SK], rb[SK], cr[SK], ckk[SK];
+    double wv[SK];
+    auto ld_raw = [&](int px) {
+        const bool pv = px >= 0 && px <= N;
+        const long long base = (long long)px * plane;
+#pragma unroll
+        for (int k = 0; k < SK; ++k) {
+            const bool v = pv && sp_valid(fl, k);
+            ra[k] = v ? src_a[base + G.noff[k]] : (V)0;
+            rb[k] = (v && two) ? src_b[base + G.noff[k]] : (V)0;
+        }
+    };
+    auto form = [&](V (&p)[SK]) {
+#pragma unroll
+        for (int k = 0; k < SK; ++k) p[k] = two ? VT::fma(beta, rb[k], ra[k]) : ra[k];
+    };
+    auto ld_coef = [&](int ex) {
+        const bool ev = ex >= 0 && ex < N;
+        const long long base = (long long)ex * eplane;
+#pragma unroll
+        for (int k = 0; k < SK; ++k) {
+            const bool v = ev && sp_elem(fl, k);
+            if constexpr (sizeof(V) == 4) {
+                const float2 c = v ? __ldg(I.coef32 + base + G.eoff[k]) : make_float2(0.f, 0.f);
+                cr[k] = c.x; ckk[k] = c.y;
+            } else {
+                const double2 c = v ? __ldg(I.coef64 + base + G.eoff[k]) : make_double2(0.0, 0.0);
+                cr[k] = c.x; ckk[k] = c.y;
+            }
+        }
+    };
+    auto ld_w = [&](int px) {
+        const bool pv = px >= xa && px <= xb;
+        const long long base = (long long)px * plane;
+#pragma unroll
+        for (int k = 0; k < SK; ++k) wv[k] = (pv && d1 && sp_out(fl, k)) ? __ldg(w + base + G.noff[k]) : 0.0;
+    };
+    auto layer = [&](int ix, int cur, V (&pc)[SK], V (&pn)[SK], V (&ac)[SK], V (&an)[SK]) {
+        const int nxt = cur ^ 1;
+        form(pn);
+#pragma unroll
+        for (int k = 0; k < SK; ++k) S.P[nxt][tid + k * ST] = pn[k];
+        ld_raw(ix + 2 <= xb + 1 ? ix + 2 : -2);
+        __syncthreads();
+        if (ix >= 0 && ix < N) {
+#pragma unroll
+            for (int k = 0; k < SK; ++k) {
+                if (!sp_elem(fl, k)) continue;
+                const int j = tid + k * ST;
+                V v[8];
+                v[0] = pc[k];
+                v[1] = S.P[cur][j + 1];
+                v[2] = S.P[cur][j + Cw];
+                v[3] = S.P[cur][j + Cw + 1];
+                v[4] = pn[k];
+                v[5] = S.P[nxt][j + 1];
+                v[6] = S.P[nxt][j + Cw];
+                v[7] = S.P[nxt][j + Cw + 1];
+                elem_wht_v<V>(v, cr[k], VT::mul(dtv, ckk[k]), cm, ck);
+                ac[k] = VT::add(ac[k], v[0]);
+                an[k] = VT::add((V)0, v[4]);
+                S.Y1[j + 1] = T2{v[1], v[5]};
+                S.Y2[j + Cw] = T2{v[2], v[6]};
+                S.Y3[j + Cw + 1] = T2{v[3], v[7]};
+            }
+        }
+        ld_coef(ix + 1 <= xb ? ix + 1 : -1);
+        __syncthreads();
+        const long long base = (long long)ix * plane;
+        const bool xbnd = ix == 0 || ix == N;
+#pragma unroll
+        for (int k = 0; k < SK; ++k) {
+            if (!sp_out(fl, k)) continue;
+            const int j = tid + k * ST;
+            const bool yzin = !sp_yzb(fl, k);
+            T2 y3{(V)0, (V)0}, y2 = y3, y1 = y3;
+            if (yzin) { y3 = S.Y3[j]; y2 = S.Y2[j]; y1 = S.Y1[j]; }
+            if (ix >= xa) {
+                const long long n = base + G.noff[k];
+                const bool bnd = !yzin || xbnd;
+                const V y = bnd ? (V)0 : VT::add(VT::add(VT::add(ac[k], y3.x), y2.x), y1.x);
+                const double pv = (double)pc[k], yd = (double)y;
+                if (loop) part[0] = dfma(pv, yd, part[0]);
+                if (d1) {
+                    part[1] = bnd ? part[1] : dadd(part[1], yd);
+                    part[2] = dfma(wv[k], pv, part[2]);
+                    part[3] = dfma(pv, pv, part[3]);
+                }
+                yout[n] = y;
+                if (loop) pout[n] = pc[k];
+            }
+            an[k] = yzin ? VT::add(VT::add(VT::add(an[k], y3.y), y2.y), y1.y) : (V)0;
+        }
+        ld_w(ix + 1);
+    };
+    ld_raw(xa - 1);
+    form(pA);
+#pragma unroll
+    for (int k = 0; k < SK; ++k) { S.P[0][tid + k * ST] = pA[k]; aA[k] = (V)0; aB[k] = (V)0; }
+    ld_raw(xa);
+    ld_coef(xa - 1);
+    for (int ix = xa - 1; ix <= xb; ++ix) {
+        layer(ix, (ix - xa + 1) & 1, pA, pB, aA, aB);
+#pragma unroll
+        for (int k = 0; k < SK; ++k) { pA[k] = pB[k]; aA[k] = aB[k]; }
+    }
+    if (!loop && !d1) return;
+    cta_tree_sum<MAXQ>(part, S.sh);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < MAXQ; ++q) B.pa[q * B.ntiles + t] = part[q];
+    }
+}
+
+// sums of one instance's partials (count values at stride qstride per quantity)
+template <int NQ>
+__device__ __forceinline__ void inst_sums(double (&v)[NQ], const double* base, long long count, long long qstride,
+                                          double (*sh)[8]) {
+    constexpr int FB = 8;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) v[q] = 0.0;
+    for (long long k0 = threadIdx.x; k0 < count; k0 += (long long)RT * FB) {
+        double t[NQ][FB];
+#pragma unroll
+        for (int q = 0; q < NQ; ++q)
+#pragma unroll
+            for (int u = 0; u < FB; ++u) {
+                const long long k = k0 + (long long)u * RT;
+                t[q][u] = (k < count) ? __ldcg(base + q * qstride + k) : 0.0;
+            }
+#pragma unroll
+        for (int q = 0; q < NQ; ++q)
+#pragma unroll
+            for (int u = 0; u < FB; ++u)
+                if (k0 + (long long)u * RT < count) v[q] = dadd(v[q], t[q][u]);
+    }
+    cta_tree_sum<NQ>(v, sh);
+}
+
+__device__ __forceinline__ double d1_rel(const double (&p)[MAXQ], double nw) {
+    const double nx = __dsqrt_rn(p[3]);
+    double rel = __ddiv_rn(fabs(dsub(p[1], p[2])), dfma(nw, nx, 1e-300));
+    if (!isfinite(rel)) rel = 1e300;
+    return rel;
+}
+
+// one block per instance: operator partials -> D1 (and alpha in the loop)
+template <int KIND>
+__global__ void __launch_bounds__(RT) kb_final_apply(BatchArgs B) {
+    __shared__ double sh[MAXQ][8];
+    const int slot = blockIdx.x;
+    if (slot >= B.n_inst) return;
+    const BInst& I = B.inst[slot];
+    if (!I.active) return;
+    BState* st = I.st;
+    if (KIND == BK_LOOP && (st->odone || st->done)) return;
+    if (KIND == BK_RESID && st->odone) return;
+    double p[MAXQ];
+    inst_sums<MAXQ>(p, B.pa + I.tile0, I.part.ntiles, B.ntiles, sh);
+    if (threadIdx.x != 0) return;
+    if (B.detect) {
+        const double rel = d1_rel(p, KIND == BK_RHS ? st->norm_wM : st->norm_wA);
+        st->d1_last = rel;
+        if (KIND == BK_LOOP) st->d1_max32 = fmax(st->d1_max32, rel);
+        else st->d1_max64 = fmax(st->d1_max64, rel);
+    }
+    if (KIND == BK_LOOP) {
+        st->applies32 += 1;
+        if (fabs(p[0]) < 1e-30) { st->broken = 1; st->done = 1; }
+        else st->alpha = __ddiv_rn(st->rho, p[0]);
+    } else {
+        st->applies64 += 1;
+    }
+}
+
+// flat block of an instance: slot, local block, first node, node count (0..KF)
+struct FlatPos { int slot; long long m0; int cnt; };
+__device__ __forceinline__ FlatPos flat_pos(const BatchArgs& B) {
+    FlatPos f{-1, 0, 0};
+    const long long g = blockIdx.x;
+    if (g >= B.nflat) return f;
+    const int slot = B.flat2inst[g];
+    if (slot < 0) return f;
+    const BInst& I = B.inst[slot];
+    const long long lb = g - I.flat0;
+    f.slot = slot;
+    f.m0 = (lb * RT + threadIdx.x) * KF;
+    const long long Nn = I.part.Nn;
+    f.cnt = (f.m0 + 1 < Nn) ? 2 : (f.m0 < Nn ? 1 : 0);
+    return f;
+}
+
+// residual r = b - A T in FP64 and the start of an inner solve:
+// r32 = r, z32 = r32 / d, d32 = 0; partials r.r, b.b (FP64), r32.z32, r32.r32
+__global__ void __launch_bounds__(RT) kb_resid(BatchArgs B) {
+    __shared__ double sh[MAXQ][8];
+    const FlatPos f = flat_pos(B);
+    double part[4] = {0.0, 0.0, 0.0, 0.0};
+    if (f.slot >= 0) {
+        const BInst& I = B.inst[f.slot];
+        if (I.active && !I.st->odone) {
+            for (int k = 0; k < f.cnt; ++k) {
+                const long long m = f.m0 + k;
+                const double bv = I.b[m];
+                const double rv = dsub(bv, I.y64[m]);
+                I.r64[m] = rv;
+                const float r32 = (float)rv;
+                const float z = __fmul_rn(r32, I.dinv32[m]);
+                I.r32[m] = r32; I.z32[m] = z; I.d32[m] = 0.f;
+                part[0] = dfma(rv, rv, part[0]);
+                part[1] = dfma(bv, bv, part[1]);
+                part[2] = dfma((double)r32, (double)z, part[2]);
+                part[3] = dfma((double)r32, (double)r32, part[3]);
+            }
+        }
+    }
+    cta_tree_sum<4>(part, sh);
+    if (threadIdx.x == 0 && blockIdx.x < B.nflat) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) B.pf[q * B.nflat + blockIdx.x] = part[q];
+    }
+}
+
+// one block per instance: outer convergence test and the inner solve's start
+__global__ void __launch_bounds__(RT) kb_outer_final(BatchArgs B) {
+    __shared__ double sh[MAXQ][8];
+    const int slot = blockIdx.x;
+    if (slot >= B.n_inst) return;
+    const BInst& I = B.inst[slot];
+    if (!I.active) return;
+    BState* st = I.st;
+    if (st->odone) return;
+    double p[4];
+    inst_sums<4>(p, B.pf + I.flat0, I.part.nflat, B.nflat, sh);
+    if (threadIdx.x != 0) return;
+    if (st->outer == 0) {
+        double bn = __dsqrt_rn(p[1]);
+        if (bn < 1e-30) bn = 1.0;
+        st->bn64 = bn;
+    }
+    st->rel64 = __ddiv_rn(__dsqrt_rn(p[0]), st->bn64);
+    const bool conv = st->rel64 < B.rtol || !(st->rel64 == st->rel64);
+    if (conv || st->outer >= B.max_outer) { st->odone = 1; st->done = 1; return; }
+    st->outer += 1;
+    st->outer_total += 1;
+    st->rho = p[2];
+    st->bn_in = __dsqrt_rn(p[3]);
+    st->iter = 0; st->broken = 0; st->beta = 0.0;
+    st->done = (st->bn_in < 1e-300) ? 1 : 0;
+}
+
+// inner FP32 update: d += alpha p, r -= alpha Ap, z = r / diag; partials r.r, r.z
+__global__ void __launch_bounds__(RT) kb_update32(BatchArgs B) {
+    __shared__ double sh[MAXQ][8];
+    const FlatPos f = flat_pos(B);
+    double part[2] = {0.0, 0.0};
+    if (f.slot >= 0) {
+        const BInst& I = B.inst[f.slot];
+        const BState* st = I.st;
+        if (I.active && !st->odone && !st->done) {
+            const int iter = st->iter;
+            const float alpha = (float)st->alpha;
+            const float* p = (iter & 1) ? I.p32b : I.p32a;
+            for (int k = 0; k < f.cnt; ++k) {
+                const long long m = f.m0 + k;
+                I.d32[m] = __fmaf_rn(alpha, p[m], I.d32[m]);
+                const float r = __fmaf_rn(-alpha, I.Ap32[m], I.r32[m]);
+                const float z = __fmul_rn(r, I.dinv32[m]);
+                I.r32[m] = r; I.z32[m] = z;
+                part[0] = dfma((double)r, (double)r, part[0]);
+                part[1] = dfma((double)r, (double)z, part[1]);
+            }
+        }
+    }
+    cta_tree_sum<2>(part, sh);
+    if (threadIdx.x == 0 && blockIdx.x < B.nflat) { B.pf[blockIdx.x] = part[0]; B.pf[B.nflat + blockIdx.x] = part[1]; }
+}
+
+// one block per instance: inner convergence and beta
+__global__ void __launch_bounds__(RT) kb_final_update32(BatchArgs B) {
+    __shared__ double sh[MAXQ][8];
+    const int slot = blockIdx.x;
+    if (slot >= B.n_inst) return;
+    const BInst& I = B.inst[slot];
+    if (!I.active) return;
+    BState* st = I.st;
+    if (st->odone || st->done) return;
+    double p[2];
+    inst_sums<2>(p, B.pf + I.flat0, I.part.nflat, B.nflat, sh);
+    if (threadIdx.x != 0) return;
+    st->inner_total += 1;
+    const double rel = __ddiv_rn(__dsqrt_rn(p[0]), st->bn_in);
+    if (rel < B.inner_tol || !(rel == rel) || st->iter + 1 >= B.max_inner) { st->done = 1; return; }
+    st->beta = __ddiv_rn(p[1], st->rho);
+    st->rho = p[1];
+    st->iter += 1;
+}
+
+// T += d (FP64) for the instances whose inner solve just finished
+__global__ void __launch_bounds__(RT) kb_correct(BatchArgs B) {
+    const FlatPos f = flat_pos(B);
+    if (f.slot < 0) return;
+    const BInst& I = B.inst[f.slot];
+    if (!I.active || I.st->odone) return;
+    for (int k = 0; k < f.cnt; ++k) {
+        const long long m = f.m0 + k;
+        I.T[m] = dadd(I.T[m], (double)I.d32[m]);
+    }
+}
+
+// set-up helpers: FP32 reciprocal of the diagonal; the interior indicator
+__global__ void k_recip32(long long n, const double* d, float* out) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = (float)__ddiv_rn(1.0, d[i]);
+}
+__global__ void k_ones_interior(int N, double* v) {
+    const long long NN = N + 1, Nn = NN * NN * NN;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < Nn; i += (long long)gridDim.x * blockDim.x)
+        v[i] = is_bnd(i, N) ? 0.0 : 1.0;
+}
+
+// step start: outer state of every active instance
+__global__ void kb_step_begin(BatchArgs B) {
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= B.n_inst) return;
+    const BInst& I = B.inst[slot];
+    if (!I.active) return;
+    BState* st = I.st;
+    st->outer = 0; st->odone = 0; st->done = 1; st->iter = 0;
+}
+
+// loop conditions: any active instance still in its outer loop (WHICH 0) /
+// in an inner solve (WHICH 1)
+template <int WHICH>
+__global__ void kb_cond(BatchArgs B, cudaGraphConditionalHandle h) {
+    int any = 0;
+    for (int s = threadIdx.x; s < B.n_inst; s += blockDim.x) {
+        const BInst& I = B.inst[s];
+        if (!I.active) continue;
+        const BState* st = I.st;
+        if (WHICH == 0 ? !st->odone : (!st->odone && !st->done)) any = 1;
+    }
+    any = __syncthreads_or(any);
+    if (threadIdx.x == 0) cudaGraphSetConditional(h, any ? 1u : 0u);
+}
+
+}  // namespace hs

@@ -1,0 +1,110 @@
+"""Batched mixed-precision solves (hs_batch_*).
+
+* Accuracy: FP32 inner solves with FP64 defect correction reach the FP64
+  solution (the oracle's PCG to 1e-13) within the outer tolerance.
+* Isolation: every reduction of an instance runs over its own tiles and
+  blocks in a fixed order, and its convergence decisions are its own, so an
+  instance gives the same bits alone, in a mixed batch, and when it joins a
+  batch that is already running (continuous batching).
+"""
+import numpy as np
+import pytest
+
+from mnhack8_b200 import _lib
+from tests.helpers import bits, field
+
+pytestmark = pytest.mark.gpu
+
+
+def gaussian_T0(oracle, N, dt, k, r):
+    return oracle.Oracle(N, dt, k, r, form="wht", no_source=True, ic="gaussian", ic_sigma=0.15).initial_condition()
+
+
+def test_mixed_precision_reaches_fp64(oracle):
+    N, dt, steps = 12, 5e-4, 6
+    k, r = field(N, "lognormal", sigma=1.5, L=0.25, seed=4)
+    o = oracle.Oracle(N, dt, k, r, form="wht", no_source=True, ic="gaussian", ic_sigma=0.15)
+    ref = o.run_case(steps, snap_every=0, tol=1e-13)["T"]
+    b = _lib.Batch(rtol=1e-10, inner_tol=1e-4)
+    s = b.add(N, dt, k, r, T0=o.initial_condition(), steps=steps)
+    while b.step()[0]:
+        pass
+    T = b.field(s)
+    inf = b.info(s)
+    b.close()
+    assert np.linalg.norm(T - ref) <= 1e-9 * np.linalg.norm(ref)
+    assert inf["steps_done"] == steps and inf["rel_residual"] < 1e-10
+    assert inf["outer_iters"] >= steps and inf["inner_iters"] > 0
+    assert inf["d1_max64"] < 1e-10                 # clean FP64 applies pass the ABFT test
+    assert 0.0 < inf["d1_max32"] < 1e-4            # FP32 applies: their rounding noise floor
+
+
+CASES = [(8, 1e-3, 4, 1), (13, 5e-4, 6, 2), (20, 2e-4, 3, 3), (5, 2e-3, 5, 4)]
+
+
+def _solo(oracle, N, dt, steps, seed, split=1):
+    k, r = field(N, "lognormal", sigma=1.0, L=0.25, seed=seed)
+    b = _lib.Batch(rtol=1e-8, tile_split=split)
+    s = b.add(N, dt, k, r, T0=gaussian_T0(oracle, N, dt, k, r), steps=steps)
+    while b.step()[0]:
+        pass
+    T, inf = b.field(s), b.info(s)
+    b.close()
+    return T, inf
+
+
+def test_alone_equals_in_the_mix(oracle):
+    solo = [_solo(oracle, *c) for c in CASES]
+    b = _lib.Batch(rtol=1e-8)
+    slots = []
+    for N, dt, steps, seed in CASES:
+        k, r = field(N, "lognormal", sigma=1.0, L=0.25, seed=seed)
+        slots.append(b.add(N, dt, k, r, T0=gaussian_T0(oracle, N, dt, k, r), steps=steps))
+    n_steps = 0
+    while b.step()[0]:
+        n_steps += 1
+    assert n_steps == max(c[2] for c in CASES)
+    for s, (T, inf) in zip(slots, solo):
+        assert np.array_equal(bits(b.field(s)), bits(T))
+        got = b.info(s)
+        assert (got["inner_iters"], got["outer_iters"]) == (inf["inner_iters"], inf["outer_iters"])
+    b.close()
+
+
+def test_join_running_batch_and_reuse_slot(oracle):
+    (N1, dt1, st1, sd1), (N2, dt2, st2, sd2), (N3, dt3, st3, sd3) = CASES[1], CASES[0], CASES[2]
+    ref1, ref2, ref3 = (_solo(oracle, *CASES[1])[0], _solo(oracle, *CASES[0])[0], _solo(oracle, *CASES[2])[0])
+    b = _lib.Batch(rtol=1e-8)
+    k, r = field(N1, "lognormal", sigma=1.0, L=0.25, seed=sd1)
+    a = b.add(N1, dt1, k, r, T0=gaussian_T0(oracle, N1, dt1, k, r), steps=st1)
+    b.step(); b.step()
+    k, r = field(N2, "lognormal", sigma=1.0, L=0.25, seed=sd2)
+    c = b.add(N2, dt2, k, r, T0=gaussian_T0(oracle, N2, dt2, k, r), steps=st2)   # joins mid-run
+    while b.info(c)["steps_left"] > 0:
+        b.step()
+    assert np.array_equal(bits(b.field(c)), bits(ref2))
+    b.remove(c)
+    k, r = field(N3, "lognormal", sigma=1.0, L=0.25, seed=sd3)
+    d = b.add(N3, dt3, k, r, T0=gaussian_T0(oracle, N3, dt3, k, r), steps=st3)  # reuses the slot
+    assert d == c
+    while b.step()[0]:
+        pass
+    assert np.array_equal(bits(b.field(a)), bits(ref1))
+    assert np.array_equal(bits(b.field(d)), bits(ref3))
+    b.close()
+
+
+def test_tile_split_changes_only_rounding(oracle):
+    T1, _ = _solo(oracle, 20, 2e-4, 3, 3, split=1)
+    T4, _ = _solo(oracle, 20, 2e-4, 3, 3, split=4)
+    assert np.linalg.norm(T1 - T4) <= 1e-7 * np.linalg.norm(T1)
+
+
+def test_bad_arguments():
+    b = _lib.Batch()
+    with pytest.raises(_lib.HeatError):
+        b.add(0, 1e-3, np.ones(1), np.ones(1))
+    with pytest.raises(_lib.HeatError):
+        b.remove(3)
+    assert b.step() == (0, 0.0)
+    b.close()
