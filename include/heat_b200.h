@@ -102,6 +102,10 @@ void        hs_default_options(hs_options* opt);
 const char* hs_last_error(void);               /* message of the last failing call on this thread */
 int         hs_api_version(void);
 void        hs_get_layout(int N, hs_layout_info* out);
+/* Gaussian initial condition of width sigma centred in the cube, the
+ * reference's --ic gaussian with a sigma parameter (het.cu:556-568), into
+ * T_host ((N+1)^3 doubles). */
+hs_status   hs_gaussian_ic(int N, double sigma, double* T_host);
 
 /* Read <prefix>_k.bin and <prefix>_rhoc.bin (N^3 float64 each) into host
  * buffers; rejects short files and non-positive/NaN values
@@ -228,9 +232,10 @@ hs_status hs_campaign(hs_solver* s, int n_steps, int snap_every, int n_flips, un
  * implicit-Euler step of every instance per hs_batch_step (one CUDA-graph
  * launch).  Each step solves (M + dt K) T = M T_old by defect correction:
  * FP64 residual r = b - A T with the ABFT checksum, an FP32 Jacobi-PCG solve
- * of A d = r to inner_tol (FP32 operator and preconditioner, FP64 dot
- * products), T += d in FP64, until ||b - A T|| / ||b|| < rtol (the true
- * residual) or max_outer corrections.  Element form wht, deterministic
+ * of A d = r (FP32 operator and preconditioner, FP64 dot products) to the
+ * relative tolerance max(inner_tol, rtol ||b|| / (2 ||r||)), T += d in FP64,
+ * until ||b - A T|| / ||b|| < rtol (the true residual) or max_outer
+ * corrections.  Element form wht, deterministic
  * scatter, Dirichlet T = 0, no source.  Instances can be added and removed
  * between steps (continuous batching). */
 typedef struct hs_batch hs_batch;
@@ -240,7 +245,7 @@ typedef struct hs_batch_options {
     int max_outer;        /* corrections per step */
     int max_inner;        /* inner PCG iterations per correction */
     int detect;           /* ABFT checksum on every operator apply */
-    int tile_split;       /* operator tiles span ceil((N+1) / tile_split) planes */
+    int tile_planes;      /* operator tiles span min(N+1, tile_planes) planes (0: 32) */
     int device;
     int pad;
 } hs_batch_options;
@@ -258,6 +263,8 @@ void      hs_batch_destroy(hs_batch* b);
  * instance takes n_steps steps.  Sets *slot. */
 hs_status hs_batch_add(hs_batch* b, int N, double dt, const double* k, const double* rhoc, const double* T0,
                        int n_steps, int* slot);
+/* level-G fault: flip bit `bit` of T[idx % (N+1)^3] before the instance's step `step` */
+hs_status hs_batch_arm_flip(hs_batch* b, int slot, int step, long long idx, int bit);
 hs_status hs_batch_remove(hs_batch* b, int slot);
 /* one step of every instance with steps left; device time of the launch */
 hs_status hs_batch_step(hs_batch* b, int* n_active, double* device_ms);

@@ -26,7 +26,7 @@ EXPORTS = [
     "hs_arm_fi", "hs_run_case", "hs_verify", "hs_solve_host", "hs_diag_cg", "hs_set_dump", "hs_set_case_tag",
     "hs_target_on_boundary", "hs_classify", "hs_cli_main", "hs_advance", "hs_set_field", "hs_get_field",
     "hs_time_kernel", "hs_dot_noalloc", "hs_campaign", "hs_batch_default_options", "hs_batch_create",
-    "hs_batch_destroy", "hs_batch_add", "hs_batch_remove", "hs_batch_step", "hs_batch_info", "hs_batch_get_field",
+    "hs_batch_destroy", "hs_batch_add", "hs_batch_arm_flip", "hs_batch_remove", "hs_batch_step", "hs_batch_info", "hs_batch_get_field", "hs_gaussian_ic",
 ]
 
 
@@ -69,7 +69,7 @@ class FlipRecord(C.Structure):
 
 class BatchOptions(C.Structure):
     _fields_ = [("rtol", C.c_double), ("inner_tol", C.c_double), ("max_outer", C.c_int), ("max_inner", C.c_int),
-                ("detect", C.c_int), ("tile_split", C.c_int), ("device", C.c_int), ("pad", C.c_int)]
+                ("detect", C.c_int), ("tile_planes", C.c_int), ("device", C.c_int), ("pad", C.c_int)]
 
 
 class BatchInstInfo(C.Structure):
@@ -158,6 +158,8 @@ def lib():
     L.hs_batch_destroy.argtypes = [vp]
     L.hs_batch_add.restype = i
     L.hs_batch_add.argtypes = [vp, i, C.c_double, vp, vp, vp, i, C.POINTER(i)]
+    L.hs_batch_arm_flip.restype = i
+    L.hs_batch_arm_flip.argtypes = [vp, i, i, C.c_longlong, i]
     L.hs_batch_remove.restype = i
     L.hs_batch_remove.argtypes = [vp, i]
     L.hs_batch_step.restype = i
@@ -166,6 +168,8 @@ def lib():
     L.hs_batch_info.argtypes = [vp, i, C.POINTER(BatchInstInfo)]
     L.hs_batch_get_field.restype = i
     L.hs_batch_get_field.argtypes = [vp, i, vp]
+    L.hs_gaussian_ic.restype = i
+    L.hs_gaussian_ic.argtypes = [i, C.c_double, vp]
     L.hs_campaign.restype = i
     L.hs_campaign.argtypes = [vp, i, i, i, C.c_ulonglong, i, C.POINTER(StepRecord), C.POINTER(FlipRecord)]
     L.hs_cli_main.restype = i
@@ -385,12 +389,12 @@ class Batch:
     """Batched mixed-precision solves (hs_batch_*): instances added to slots
     advance one implicit-Euler step per step() call, all in one graph launch."""
 
-    def __init__(self, rtol=1e-8, inner_tol=1e-4, max_outer=10, max_inner=500, detect=True, tile_split=1,
+    def __init__(self, rtol=1e-8, inner_tol=1e-4, max_outer=10, max_inner=500, detect=True, tile_planes=32,
                  device=0):
         o = BatchOptions()
         lib().hs_batch_default_options(C.byref(o))
         o.rtol, o.inner_tol, o.max_outer, o.max_inner = rtol, inner_tol, max_outer, max_inner
-        o.detect, o.tile_split, o.device = int(detect), int(tile_split), int(device)
+        o.detect, o.tile_planes, o.device = int(detect), int(tile_planes), int(device)
         self._h = C.c_void_p()
         check(lib().hs_batch_create(C.byref(o), C.byref(self._h)))
         self.Nn = {}
@@ -403,6 +407,10 @@ class Batch:
                                  T0.ctypes.data if T0 is not None else None, int(steps), C.byref(slot)))
         self.Nn[slot.value] = (N + 1) ** 3
         return slot.value
+
+    def arm_flip(self, slot, step, idx, bit):
+        """Flip bit `bit` of the field entry idx before the instance's step `step`."""
+        check(lib().hs_batch_arm_flip(self._h, int(slot), int(step), int(idx), int(bit)))
 
     def remove(self, slot):
         check(lib().hs_batch_remove(self._h, int(slot)))
@@ -434,6 +442,13 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def gaussian_ic(N, sigma=0.15):
+    """The library's Gaussian initial condition ((N+1)^3 doubles)."""
+    T = np.empty((N + 1) ** 3)
+    check(lib().hs_gaussian_ic(int(N), float(sigma), T.ctypes.data))
+    return T
 
 
 def dot_noalloc(N, x_dev, y_dev, out_dev):

@@ -20,9 +20,9 @@
 namespace {
 
 // tile shape of one batched instance: C, R as in the slab layout (largest
-// tile plane that fits, fewest positions loaded per node), planes per tile
-// CX = ceil((N+1) / split)
-Part batch_part(int N, int split) {
+// tile plane that fits, fewest positions loaded per node), CX = min(N+1,
+// planes) planes per tile
+Part batch_part(int N, int planes) {
     const long long NN = N + 1;
     long long bestC = NN, bestR = 1, best_cost = -1;
     const long long cmin = NN < 30 ? NN : 30;
@@ -35,9 +35,8 @@ Part batch_part(int N, int split) {
         const long long cost = NCB * NRB * (Cw * (R + 2) + 2 * (C + 1) * (R + 1));
         if (best_cost < 0 || cost < best_cost) { best_cost = cost; bestC = C; bestR = R; }
     }
-    if (split < 1) split = 1;
-    long long CX = (NN + split - 1) / split;
-    if (CX < 1) CX = 1;
+    if (planes < 1) planes = 32;
+    const long long CX = planes < NN ? planes : NN;
     Part p{};
     p.N = N; p.NN = (int)NN;
     p.C = (int)bestC; p.R = (int)bestR; p.CX = (int)CX;
@@ -61,6 +60,8 @@ struct hs_batch {
         int N = 0;
         double dt = 0;
         int steps_left = 0, steps_done = 0;
+        int flip_step = -1, flip_bit = 0;   // armed level-G flip (T[flip_idx] before step flip_step)
+        long long flip_idx = 0;
         Part part{};
         void* mem = nullptr;      // one allocation holding every buffer of the instance
         BInst desc{};
@@ -230,15 +231,15 @@ void hs_batch_default_options(hs_batch_options* o) {
     if (!o) return;
     std::memset(o, 0, sizeof(*o));
     o->rtol = 1e-8; o->inner_tol = 1e-4; o->max_outer = 10; o->max_inner = 500;
-    o->detect = 1; o->tile_split = 1; o->device = 0;
+    o->detect = 1; o->tile_planes = 32; o->device = 0;
 }
 
 hs_status hs_batch_create(const hs_batch_options* opt, hs_batch** out) {
     if (!opt || !out) { set_error("bad arguments"); return HS_ERR_ARG; }
     *out = nullptr;
     if (!(opt->rtol > 0) || !(opt->inner_tol > 0) || opt->max_outer < 1 || opt->max_inner < 1 ||
-        opt->tile_split < 1) {
-        set_error("hs_batch_create: rtol, inner_tol > 0; max_outer, max_inner, tile_split >= 1");
+        opt->tile_planes < 0) {
+        set_error("hs_batch_create: rtol, inner_tol > 0; max_outer, max_inner >= 1; tile_planes >= 0");
         return HS_ERR_ARG;
     }
     HS_CUDA(cudaSetDevice(opt->device));
@@ -365,12 +366,23 @@ hs_status hs_batch_add(hs_batch* b, int N, double dt, const double* k, const dou
     HS_CUDA(cudaMemcpyAsync(b->d_st.p + slot, &st0, sizeof(BState), cudaMemcpyHostToDevice, b->s));
     HS_CUDA(cudaStreamSynchronize(b->s));
     sl.used = true; sl.N = N; sl.dt = dt; sl.steps_left = n_steps; sl.steps_done = 0;
-    sl.part = batch_part(N, b->opt.tile_split);
+    sl.part = batch_part(N, b->opt.tile_planes);
     d.part = sl.part;
     sl.mem = mem;
     sl.desc = d;
     b->dirty = true;
     if (slot_out) *slot_out = slot;
+    return HS_OK;
+}
+
+hs_status hs_batch_arm_flip(hs_batch* b, int slot, int step, long long idx, int bit) {
+    if (!b || slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot].used || step < 0 || idx < 0 ||
+        bit < 0 || bit > 63) {
+        set_error("hs_batch_arm_flip: bad arguments");
+        return HS_ERR_ARG;
+    }
+    auto& sl = b->slots[slot];
+    sl.flip_step = step; sl.flip_idx = idx % sl.part.Nn; sl.flip_bit = bit;
     return HS_OK;
 }
 
@@ -406,6 +418,10 @@ hs_status hs_batch_step(hs_batch* b, int* n_active, double* device_ms) {
     }
     hs_status st = build_batch_graph(b);
     if (st != HS_OK) return st;
+    // armed flips of this step (level G: one bit of the field before the step)
+    for (auto& sl : b->slots)
+        if (sl.used && sl.steps_left > 0 && sl.flip_step == sl.steps_done)
+            k_flip<<<1, 1, 0, b->s>>>(sl.desc.T, sl.flip_idx, sl.flip_bit);
     cudaEvent_t e0, e1;
     HS_CUDA(cudaEventCreate(&e0));
     HS_CUDA(cudaEventCreate(&e1));

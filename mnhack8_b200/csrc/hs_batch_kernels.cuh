@@ -15,7 +15,7 @@ namespace hs {
 // per-instance scalars, device resident
 struct BState {
     // inner FP32 PCG
-    double rho, alpha, beta, bn_in;
+    double rho, alpha, beta, bn_in, tol_in;
     int iter, done, broken, pad0;
     // outer defect correction
     double bn64, rel64, d1_last, d1_max64, d1_max32;
@@ -418,6 +418,8 @@ __global__ void __launch_bounds__(RT) kb_outer_final(BatchArgs B) {
     st->outer_total += 1;
     st->rho = p[2];
     st->bn_in = __dsqrt_rn(p[3]);
+    // solve only as far as the outer target needs: max(inner_tol, rtol / (2 rel64))
+    st->tol_in = fmax(B.inner_tol, __ddiv_rn(0.5 * B.rtol, st->rel64));
     st->iter = 0; st->broken = 0; st->beta = 0.0;
     st->done = (st->bn_in < 1e-300) ? 1 : 0;
 }
@@ -463,7 +465,7 @@ __global__ void __launch_bounds__(RT) kb_final_update32(BatchArgs B) {
     if (threadIdx.x != 0) return;
     st->inner_total += 1;
     const double rel = __ddiv_rn(__dsqrt_rn(p[0]), st->bn_in);
-    if (rel < B.inner_tol || !(rel == rel) || st->iter + 1 >= B.max_inner) { st->done = 1; return; }
+    if (rel < st->tol_in || !(rel == rel) || st->iter + 1 >= B.max_inner) { st->done = 1; return; }
     st->beta = __ddiv_rn(p[1], st->rho);
     st->rho = p[1];
     st->iter += 1;

@@ -325,6 +325,12 @@ void hs_get_layout(int N, hs_layout_info* out) {
     out->cx = L.CX; out->ty = L.R; out->tz = L.C; out->rt = RT; out->bpt = SK; out->kf = KF;
 }
 
+hs_status hs_gaussian_ic(int N, double sigma, double* T_host) {
+    if (N < 1 || N > 1200 || !(sigma > 0) || !T_host) { set_error("hs_gaussian_ic: bad arguments"); return HS_ERR_ARG; }
+    gaussian_ic(N, sigma, T_host);
+    return HS_OK;
+}
+
 void hs_default_options(hs_options* o) {
     if (!o) return;
     std::memset(o, 0, sizeof(*o));

@@ -1,0 +1,303 @@
+"""Precision, batching and serving forms of the transient-heat solve.
+
+Each subcommand times the batched mixed-precision solver (FP32 inner PCG,
+FP64 defect correction on the true residual, hs_batch_*) beside the plain
+FP64 drop-in (hs_solver: FP64 Jacobi-PCG, one solve at a time) on the same
+GPU and the same seeded synthetic inputs, and prints one JSON line.
+
+  precision  one N=256 solve: lognormal k (sigma 1.5, correlation 16
+             elements), 20 steps to rtol 1e-8; error of both against an
+             FP64 solve at rtol 1e-12, ABFT noise floors of both precisions.
+  batching   an ensemble of independent solves (default 256, N uniform in
+             16..96, lognormal k sigma 1 with correlation N/8 elements),
+             20 steps each to rtol 1e-8, all in one batch (one graph launch
+             per step); the tile depth is chosen by a short autotuning run.
+  serving    a seeded Poisson stream of requests (N uniform in 16..160, steps
+             uniform in 10..100, 30 % with one seeded bit flip of the field),
+             served by continuous batching: requests join the running batch
+             as they arrive and leave when done; p50 / p99 latency and
+             solves/s beside serial plain FP64 serving of the same stream.
+
+Fields are generated before the timed regions (the reference generator's
+algorithm, host NumPy); every timed region holds solver work only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+from mnhack8_b200 import _lib  # noqa: E402
+from mnhack8_b200.fields import FieldSpec, make_field  # noqa: E402
+
+DT = 1e-4
+IC_SIGMA = 0.15
+
+
+def lognormal(N, sigma, corr_elements, seed):
+    k, r, _ = make_field(FieldSpec(n=N, model="lognormal", mu=0.0, sigma=sigma, L=corr_elements / N, seed=seed))
+    return k.ravel(), r.ravel()
+
+
+def _lognormal_job(args):
+    return lognormal(*args)
+
+
+def lognormal_many(jobs, workers=None):
+    """Fields for (N, sigma, corr_elements, seed) jobs, generated in a process pool
+    (spawned, so no worker inherits a CUDA context)."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    workers = workers or max(1, min(16, (os.cpu_count() or 2) - 1))
+    with cf.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+        return list(ex.map(_lognormal_job, jobs, chunksize=4))
+
+
+def batch_bytes(N):
+    """Device bytes of one batched instance (the allocation hs_batch_add makes)."""
+    Nn, Ne = (N + 1) ** 3, N ** 3
+    return 7 * 8 * Nn + 7 * 4 * Nn + 48 * Ne + 16 * 256
+
+
+def fp64_solve(N, k, r, steps, rtol, device=0):
+    """Plain FP64 drop-in: steps implicit-Euler steps from the Gaussian IC;
+    returns (field, CG iterations, device ms)."""
+    g = _lib.Solver(N, DT, k, r, kernel="wht", scatter="colored", detect=True, no_source=True, ic="gaussian",
+                    ic_sigma=IC_SIGMA, rtol=rtol, max_iter=1000, device=device)
+    it, ms = g.advance(steps, from_ic=True)
+    T = g.get_field()
+    g.close()
+    return T, it, ms
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+# ---- config 3 --------------------------------------------------------------------
+def precision(N=256, steps=20, rtol=1e-8, inner_tol=1e-4, sigma=1.5, corr=16.0, seed=3, device=0):
+    (k, r), = lognormal_many([(N, sigma, corr, seed)], workers=1)
+    T0 = _lib.gaussian_ic(N, IC_SIGMA)
+    T_ref, it_ref, _ = fp64_solve(N, k, r, steps, 1e-12, device)
+    fp64_solve(N, k, r, 2, rtol, device)                     # warm-up
+    T64, it64, ms64 = fp64_solve(N, k, r, steps, rtol, device)
+    b = _lib.Batch(rtol=rtol, inner_tol=inner_tol, device=device)
+    w = b.add(N, DT, k, r, T0=T0, steps=2)                   # warm-up (graph capture)
+    while b.step()[0]:
+        pass
+    b.remove(w)
+    s = b.add(N, DT, k, r, T0=T0, steps=steps)
+    ms_mixed = 0.0
+    while True:
+        n, ms = b.step()
+        if not n:
+            break
+        ms_mixed += ms
+    Tm, inf = b.field(s), b.info(s)
+    b.close()
+    nodes = (N + 1) ** 3
+    return {
+        "form": "precision", "N": N, "nodes": nodes, "steps": steps, "rtol": rtol, "inner_tol": inner_tol,
+        "field": f"lognormal sigma {sigma}, correlation {corr:g} elements, seed {seed}",
+        "fp64": {"ms": ms64, "cg_iters": it64, "err_vs_fp64_1e-12": rel(T64, T_ref),
+                 "solves_per_s": 1e3 / ms64},
+        "mixed": {"ms": ms_mixed, "inner_iters": inf["inner_iters"], "outer_iters": inf["outer_iters"],
+                  "err_vs_fp64_1e-12": rel(Tm, T_ref), "final_true_rel_residual": inf["rel_residual"],
+                  "solves_per_s": 1e3 / ms_mixed},
+        "speedup_mixed_vs_fp64": ms64 / ms_mixed,
+        "abft_noise_floor": {"fp64_applies_max_d1": inf["d1_max64"], "fp32_applies_max_d1": inf["d1_max32"],
+                             "fp64_threshold": 1e-10},
+        "reference_cg_iters_at_1e-12": it_ref,
+    }
+
+
+# ---- config 4 --------------------------------------------------------------------
+def ensemble_specs(n, nmin, nmax, seed):
+    rng = np.random.default_rng(seed)
+    Ns = rng.integers(nmin, nmax + 1, size=n)
+    return [(int(N), 1000 + i) for i, N in enumerate(Ns)]
+
+
+def run_batch(fields, steps, rtol, inner_tol, planes, device=0):
+    b = _lib.Batch(rtol=rtol, inner_tol=inner_tol, tile_planes=planes, device=device)
+    slots = [b.add(N, DT, k, r, T0=T0, steps=steps) for (N, k, r, T0) in fields]
+    tot = 0.0
+    while True:
+        n, ms = b.step()
+        if not n:
+            break
+        tot += ms
+    infos = [b.info(s) for s in slots]
+    b.close()
+    return tot, infos
+
+
+def batching(n=256, nmin=16, nmax=96, steps=20, rtol=1e-8, inner_tol=1e-4, seed=7, serial_sample=None, device=0):
+    specs = ensemble_specs(n, nmin, nmax, seed)
+    kr = lognormal_many([(N, 1.0, N / 8.0, sd) for N, sd in specs])
+    fields = [(N, k, r, _lib.gaussian_ic(N, IC_SIGMA)) for (N, _), (k, r) in zip(specs, kr)]
+    # autotuner: planes per operator tile, timed on 2 steps of the first 64 instances
+    tune = {}
+    for planes in (8, 16, 32, 96):
+        run_batch(fields[:64], 1, rtol, inner_tol, planes, device)         # capture / warm
+        ms, _ = run_batch(fields[:64], 2, rtol, inner_tol, planes, device)
+        tune[planes] = ms
+    best = min(tune, key=tune.get)
+    ms_b, infos = run_batch(fields, steps, rtol, inner_tol, best, device)
+    # serial plain FP64, one solve after another (all, or a sample scaled up)
+    idx = range(len(specs)) if not serial_sample else range(min(serial_sample, len(specs)))
+    fp64_solve(fields[0][0], fields[0][1], fields[0][2], 2, rtol, device)  # warm-up
+    ms_s, n_s = 0.0, 0
+    for i in idx:
+        N, k, r, _ = fields[i]
+        _, _, ms = fp64_solve(N, k, r, steps, rtol, device)
+        ms_s += ms
+        n_s += 1
+    ms_serial = ms_s * len(specs) / n_s
+    dof_it = sum((N + 1) ** 3 * inf["inner_iters"] for (N, _, _, _), inf in zip(fields, infos))
+    return {
+        "form": "batching", "instances": n, "N_range": [nmin, nmax], "steps": steps, "rtol": rtol,
+        "inner_tol": inner_tol, "autotune_ms_per_tile_planes": tune, "tile_planes": best,
+        "batch_ms": ms_b, "batch_solves_per_s": n / (ms_b * 1e-3),
+        "batch_fp32_dof_iters_per_s": dof_it / (ms_b * 1e-3),
+        "max_final_true_rel_residual": max(inf["rel_residual"] for inf in infos),
+        "serial_fp64_ms": ms_serial, "serial_fp64_solves_per_s": n / (ms_serial * 1e-3),
+        "serial_fp64_timed_solves": n_s,
+        "speedup_vs_serial_fp64": ms_serial / ms_b,
+    }
+
+
+# ---- config 5 --------------------------------------------------------------------
+def request_stream(n, rate, seed, nmin=16, nmax=160, smin=10, smax=100, flip_frac=0.3):
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, size=n))
+    reqs = []
+    for i in range(n):
+        N = int(rng.integers(nmin, nmax + 1))
+        steps = int(rng.integers(smin, smax + 1))
+        flip = None
+        if rng.random() < flip_frac:
+            flip = (int(rng.integers(0, steps)), int(rng.integers(0, (N + 1) ** 3)), int(rng.integers(0, 64)))
+        reqs.append(dict(id=i, t=float(t[i]), N=N, steps=steps, flip=flip, seed=5000 + i))
+    return reqs
+
+
+def serving(n=400, rate=200.0, seed=11, rtol=1e-8, inner_tol=1e-4, max_live=64, hbm_fraction=0.5, device=0):
+    import torch
+    reqs = request_stream(n, rate, seed)
+    kr = lognormal_many([(q["N"], 1.0, q["N"] / 8.0, q["seed"]) for q in reqs])
+    for q, (k, r) in zip(reqs, kr):
+        q["k"], q["r"] = k, r
+        q["T0"] = _lib.gaussian_ic(q["N"], IC_SIGMA)
+    # admission by free HBM: the live instances' bytes stay within this budget
+    free, _ = torch.cuda.mem_get_info(device)
+    budget = int(hbm_fraction * free)
+    # continuous batching on a wall clock
+    b = _lib.Batch(rtol=rtol, inner_tol=inner_tol, device=device)
+    w = b.add(16, DT, np.ones(16 ** 3), np.ones(16 ** 3), steps=1)   # graph capture
+    b.step()
+    b.remove(w)
+    lat, live, queue = {}, {}, list(reqs)
+    live_bytes, peak_live = 0, 0
+    t0 = time.perf_counter()
+    while queue or live:
+        now = time.perf_counter() - t0
+        while (queue and queue[0]["t"] <= now and len(live) < max_live and
+               live_bytes + batch_bytes(queue[0]["N"]) <= budget):
+            q = queue.pop(0)
+            live_bytes += batch_bytes(q["N"])
+            s = b.add(q["N"], DT, q["k"], q["r"], T0=q["T0"], steps=q["steps"])
+            if q["flip"]:
+                b.arm_flip(s, *q["flip"])
+            q["left"] = q["steps"]
+            live[s] = q
+        peak_live = max(peak_live, len(live))
+        if not live:
+            time.sleep(max(0.0, queue[0]["t"] - (time.perf_counter() - t0)))
+            continue
+        b.step()
+        done_at = time.perf_counter() - t0
+        for q in live.values():
+            q["left"] -= 1
+        for s in [s for s, q in live.items() if q["left"] == 0]:
+            q = live.pop(s)
+            live_bytes -= batch_bytes(q["N"])
+            lat[q["id"]] = done_at - q["t"]
+            b.remove(s)
+    wall_b = time.perf_counter() - t0
+    b.close()
+    # serial plain FP64: the same stream, one solve at a time
+    lat_s = {}
+    t0 = time.perf_counter()
+    busy_until = 0.0
+    for q in reqs:
+        while time.perf_counter() - t0 < q["t"]:
+            time.sleep(min(1e-3, q["t"] - (time.perf_counter() - t0)))
+        g = _lib.Solver(q["N"], DT, q["k"], q["r"], kernel="wht", scatter="colored", detect=True, no_source=True,
+                        ic="gaussian", ic_sigma=IC_SIGMA, rtol=rtol, max_iter=1000, device=device)
+        g.advance(0, from_ic=True)
+        if q["flip"]:
+            fs, fi, fb = q["flip"]
+            if fs > 0:
+                g.advance(fs, from_ic=False)
+            T = g.get_field()
+            T.view(np.uint64)[fi] ^= np.uint64(1) << np.uint64(fb)
+            g.set_field(T)
+            g.advance(q["steps"] - fs, from_ic=False)
+        else:
+            g.advance(q["steps"], from_ic=False)
+        g.close()
+        busy_until = time.perf_counter() - t0
+        lat_s[q["id"]] = busy_until - q["t"]
+    wall_s = time.perf_counter() - t0
+
+    def pct(d, p):
+        return float(np.percentile(np.array(list(d.values())), p))
+
+    return {
+        "form": "serving", "requests": n, "rate_per_s": rate, "N_range": [16, 160], "steps_range": [10, 100],
+        "flip_fraction": 0.3, "rtol": rtol, "max_live": max_live, "hbm_budget_bytes": budget,
+        "peak_live": peak_live,
+        "batched": {"wall_s": wall_b, "solves_per_s": n / wall_b, "p50_latency_s": pct(lat, 50),
+                    "p99_latency_s": pct(lat, 99)},
+        "serial_fp64": {"wall_s": wall_s, "solves_per_s": n / wall_s, "p50_latency_s": pct(lat_s, 50),
+                        "p99_latency_s": pct(lat_s, 99)},
+        "throughput_ratio": (n / wall_b) / (n / wall_s),
+    }
+
+
+def _main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    p = sub.add_parser("precision")
+    p.add_argument("--N", type=int, default=256)
+    p.add_argument("--steps", type=int, default=20)
+    p = sub.add_parser("batching")
+    p.add_argument("--n", type=int, default=256)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--serial-sample", type=int, default=None)
+    p = sub.add_parser("serving")
+    p.add_argument("--n", type=int, default=400)
+    p.add_argument("--rate", type=float, default=200.0)
+    p.add_argument("--max-live", type=int, default=64)
+    a = ap.parse_args(argv)
+    if a.cmd == "precision":
+        out = precision(N=a.N, steps=a.steps)
+    elif a.cmd == "batching":
+        out = batching(n=a.n, steps=a.steps, serial_sample=a.serial_sample)
+    else:
+        out = serving(n=a.n, rate=a.rate, max_live=a.max_live)
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(_main())

@@ -42,9 +42,9 @@ def test_mixed_precision_reaches_fp64(oracle):
 CASES = [(8, 1e-3, 4, 1), (13, 5e-4, 6, 2), (20, 2e-4, 3, 3), (5, 2e-3, 5, 4)]
 
 
-def _solo(oracle, N, dt, steps, seed, split=1):
+def _solo(oracle, N, dt, steps, seed, planes=32):
     k, r = field(N, "lognormal", sigma=1.0, L=0.25, seed=seed)
-    b = _lib.Batch(rtol=1e-8, tile_split=split)
+    b = _lib.Batch(rtol=1e-8, tile_planes=planes)
     s = b.add(N, dt, k, r, T0=gaussian_T0(oracle, N, dt, k, r), steps=steps)
     while b.step()[0]:
         pass
@@ -94,9 +94,9 @@ def test_join_running_batch_and_reuse_slot(oracle):
     b.close()
 
 
-def test_tile_split_changes_only_rounding(oracle):
-    T1, _ = _solo(oracle, 20, 2e-4, 3, 3, split=1)
-    T4, _ = _solo(oracle, 20, 2e-4, 3, 3, split=4)
+def test_tile_depth_changes_only_rounding(oracle):
+    T1, _ = _solo(oracle, 20, 2e-4, 3, 3, planes=32)
+    T4, _ = _solo(oracle, 20, 2e-4, 3, 3, planes=5)
     assert np.linalg.norm(T1 - T4) <= 1e-7 * np.linalg.norm(T1)
 
 
