@@ -233,9 +233,10 @@ hs_status hs_campaign(hs_solver* s, int n_steps, int snap_every, int n_flips, un
  * launch).  Each step solves (M + dt K) T = M T_old by defect correction:
  * FP64 residual r = b - A T with the ABFT checksum, an FP32 Jacobi-PCG solve
  * of A d = r (FP32 operator and preconditioner, FP64 dot products) to the
- * relative tolerance max(inner_tol, rtol ||b|| / (2 ||r||)), T += d in FP64,
- * until ||b - A T|| / ||b|| < rtol (the true residual) or max_outer
- * corrections.  Element form wht, deterministic
+ * relative tolerance max(inner_tol, rtol ||b|| / (2 ||r||)), T += d in FP64
+ * at the interior nodes (a correction whose inner solve went non-finite is
+ * discarded and re-solved), until ||b - A T|| / ||b|| < rtol (the true
+ * residual) or max_outer corrections.  Element form wht, deterministic
  * scatter, Dirichlet T = 0, no source.  Instances can be added and removed
  * between steps (continuous batching). */
 typedef struct hs_batch hs_batch;
@@ -252,6 +253,10 @@ typedef struct hs_batch_options {
 typedef struct hs_batch_inst_info {
     int N, steps_done, steps_left, pad;
     long long inner_iters, outer_iters, applies32, applies64, tiles;
+    int fault_fired;      /* an armed vector fault has fired */
+    int stalls;           /* steps that ended at max_outer without reaching rtol */
+    int inner_faults;     /* inner solves that went non-finite (correction discarded) */
+    int pad2;
     double rel_residual;  /* last true relative residual */
     double d1_max64;      /* largest D1 of the FP64 applies */
     double d1_max32;      /* largest D1 of the FP32 applies (their noise floor when clean) */
@@ -265,6 +270,11 @@ hs_status hs_batch_add(hs_batch* b, int N, double dt, const double* k, const dou
                        int n_steps, int* slot);
 /* level-G fault: flip bit `bit` of T[idx % (N+1)^3] before the instance's step `step` */
 hs_status hs_batch_arm_flip(hs_batch* b, int slot, int step, long long idx, int bit);
+/* fault in an FP32 inner vector: level HS_FI_P (p after formation), HS_FI_RV
+ * (r after its update) or HS_FI_AP (Ap after projection), entry idx, bit 0..31,
+ * in step `step`, correction `outer` (1-based), inner iteration `iter` */
+typedef struct hs_batch_fault { int level, step, outer, iter; long long idx; int bit, pad; } hs_batch_fault;
+hs_status hs_batch_arm_fault(hs_batch* b, int slot, const hs_batch_fault* f);
 hs_status hs_batch_remove(hs_batch* b, int slot);
 /* one step of every instance with steps left; device time of the launch */
 hs_status hs_batch_step(hs_batch* b, int* n_active, double* device_ms);

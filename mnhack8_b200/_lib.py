@@ -26,7 +26,7 @@ EXPORTS = [
     "hs_arm_fi", "hs_run_case", "hs_verify", "hs_solve_host", "hs_diag_cg", "hs_set_dump", "hs_set_case_tag",
     "hs_target_on_boundary", "hs_classify", "hs_cli_main", "hs_advance", "hs_set_field", "hs_get_field",
     "hs_time_kernel", "hs_dot_noalloc", "hs_campaign", "hs_batch_default_options", "hs_batch_create",
-    "hs_batch_destroy", "hs_batch_add", "hs_batch_arm_flip", "hs_batch_remove", "hs_batch_step", "hs_batch_info", "hs_batch_get_field", "hs_gaussian_ic",
+    "hs_batch_destroy", "hs_batch_add", "hs_batch_arm_flip", "hs_batch_arm_fault", "hs_batch_remove", "hs_batch_step", "hs_batch_info", "hs_batch_get_field", "hs_gaussian_ic",
 ]
 
 
@@ -72,10 +72,16 @@ class BatchOptions(C.Structure):
                 ("detect", C.c_int), ("tile_planes", C.c_int), ("device", C.c_int), ("pad", C.c_int)]
 
 
+class BatchFault(C.Structure):
+    _fields_ = [("level", C.c_int), ("step", C.c_int), ("outer", C.c_int), ("iter", C.c_int), ("idx", C.c_longlong),
+                ("bit", C.c_int), ("pad", C.c_int)]
+
+
 class BatchInstInfo(C.Structure):
     _fields_ = [("N", C.c_int), ("steps_done", C.c_int), ("steps_left", C.c_int), ("pad", C.c_int),
                 ("inner_iters", C.c_longlong), ("outer_iters", C.c_longlong), ("applies32", C.c_longlong),
-                ("applies64", C.c_longlong), ("tiles", C.c_longlong), ("rel_residual", C.c_double),
+                ("applies64", C.c_longlong), ("tiles", C.c_longlong), ("fault_fired", C.c_int),
+                ("stalls", C.c_int), ("inner_faults", C.c_int), ("pad2", C.c_int), ("rel_residual", C.c_double),
                 ("d1_max64", C.c_double), ("d1_max32", C.c_double)]
 
 
@@ -160,6 +166,8 @@ def lib():
     L.hs_batch_add.argtypes = [vp, i, C.c_double, vp, vp, vp, i, C.POINTER(i)]
     L.hs_batch_arm_flip.restype = i
     L.hs_batch_arm_flip.argtypes = [vp, i, i, C.c_longlong, i]
+    L.hs_batch_arm_fault.restype = i
+    L.hs_batch_arm_fault.argtypes = [vp, i, C.POINTER(BatchFault)]
     L.hs_batch_remove.restype = i
     L.hs_batch_remove.argtypes = [vp, i]
     L.hs_batch_step.restype = i
@@ -412,6 +420,12 @@ class Batch:
         """Flip bit `bit` of the field entry idx before the instance's step `step`."""
         check(lib().hs_batch_arm_flip(self._h, int(slot), int(step), int(idx), int(bit)))
 
+    def arm_fault(self, slot, level, step, outer, it, idx, bit):
+        """Flip bit `bit` (0..31) of an FP32 inner vector entry: level 'P', 'RV' or
+        'AP' (or 5/6/7), in step `step`, correction `outer` (1-based), inner iteration `it`."""
+        f = BatchFault(LEVELS.get(level, level), int(step), int(outer), int(it), int(idx), int(bit), 0)
+        check(lib().hs_batch_arm_fault(self._h, int(slot), C.byref(f)))
+
     def remove(self, slot):
         check(lib().hs_batch_remove(self._h, int(slot)))
         self.Nn.pop(slot, None)
@@ -425,7 +439,7 @@ class Batch:
     def info(self, slot):
         r = BatchInstInfo()
         check(lib().hs_batch_info(self._h, int(slot), C.byref(r)))
-        return {name: getattr(r, name) for name, _ in BatchInstInfo._fields_ if name != "pad"}
+        return {name: getattr(r, name) for name, _ in BatchInstInfo._fields_ if name not in ("pad", "pad2")}
 
     def field(self, slot):
         T = np.empty(self.Nn[slot])

@@ -9,7 +9,8 @@
 //   while not converged (bounded by max_outer):
 //       FP32 Jacobi-PCG on A d = r to inner_tol (bounded by max_inner),
 //       every launch covering the tiles of all instances still iterating;
-//       T += d (FP64); r = b - A T; test.
+//       T += d (FP64, interior nodes; discarded if the inner solve went
+//       non-finite); r = b - A T; test.
 // Instances are added and removed between steps (continuous batching): the
 // host compacts their tile and block ranges into device maps that the graph
 // reads, so the graph stays valid until the capacity has to grow.
@@ -62,6 +63,7 @@ struct hs_batch {
         int steps_left = 0, steps_done = 0;
         int flip_step = -1, flip_bit = 0;   // armed level-G flip (T[flip_idx] before step flip_step)
         long long flip_idx = 0;
+        hs_batch_fault fault{};             // armed vector fault (level 5/6/7, FP32 inner vectors)
         Part part{};
         void* mem = nullptr;      // one allocation holding every buffer of the instance
         BInst desc{};
@@ -212,6 +214,7 @@ hs_status build_batch_graph(hs_batch* b) {
     cudaGraph_t otail;
     HS_CUDA(cudaStreamBeginCapture(b->s, cudaStreamCaptureModeThreadLocal));
     kb_correct<<<(int)a.nflat, RT, 0, b->s>>>(a);
+    kb_count_bad<<<(a.n_inst + 127) / 128, 128, 0, b->s>>>(a);
     enqueue_resid(b, a);
     kb_cond<0><<<1, 1024, 0, b->s>>>(a, c_out);
     HS_CUDA(cudaStreamEndCapture(b->s, &otail));
@@ -386,6 +389,19 @@ hs_status hs_batch_arm_flip(hs_batch* b, int slot, int step, long long idx, int 
     return HS_OK;
 }
 
+hs_status hs_batch_arm_fault(hs_batch* b, int slot, const hs_batch_fault* f) {
+    if (!b || !f || slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot].used || f->step < 0 ||
+        f->outer < 1 || f->iter < 0 || f->idx < 0 || f->bit < 0 || f->bit > 31 ||
+        (f->level != HS_FI_P && f->level != HS_FI_RV && f->level != HS_FI_AP)) {
+        set_error("hs_batch_arm_fault: level 5/6/7, step >= 0, outer >= 1, iter >= 0, bit 0..31");
+        return HS_ERR_ARG;
+    }
+    auto& sl = b->slots[slot];
+    sl.fault = *f;
+    sl.fault.idx = f->idx % sl.part.Nn;
+    return HS_OK;
+}
+
 hs_status hs_batch_remove(hs_batch* b, int slot) {
     if (!b || slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot].used) {
         set_error("hs_batch_remove: no such instance");
@@ -419,9 +435,13 @@ hs_status hs_batch_step(hs_batch* b, int* n_active, double* device_ms) {
     hs_status st = build_batch_graph(b);
     if (st != HS_OK) return st;
     // armed flips of this step (level G: one bit of the field before the step)
-    for (auto& sl : b->slots)
-        if (sl.used && sl.steps_left > 0 && sl.flip_step == sl.steps_done)
-            k_flip<<<1, 1, 0, b->s>>>(sl.desc.T, sl.flip_idx, sl.flip_bit);
+    for (auto& sl : b->slots) {
+        if (!sl.used || sl.steps_left <= 0) continue;
+        if (sl.flip_step == sl.steps_done) k_flip<<<1, 1, 0, b->s>>>(sl.desc.T, sl.flip_idx, sl.flip_bit);
+        if (sl.fault.level && sl.fault.step == sl.steps_done)
+            kb_arm<<<1, 1, 0, b->s>>>(sl.desc.st, sl.fault.level, sl.fault.outer, sl.fault.iter, sl.fault.idx,
+                                      sl.fault.bit);
+    }
     cudaEvent_t e0, e1;
     HS_CUDA(cudaEventCreate(&e0));
     HS_CUDA(cudaEventCreate(&e1));
@@ -430,6 +450,9 @@ hs_status hs_batch_step(hs_batch* b, int* n_active, double* device_ms) {
     HS_CUDA(cudaEventRecord(e1, b->s));
     HS_CUDA(cudaEventSynchronize(e1));
     HS_CUDA(cudaGetLastError());
+    for (auto& sl : b->slots)
+        if (sl.used && sl.steps_left > 0 && sl.fault.level && sl.fault.step == sl.steps_done)
+            kb_arm<<<1, 1, 0, b->s>>>(sl.desc.st, 0, 0, 0, 0, 0);
     float ms = 0.f;
     cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0); cudaEventDestroy(e1);
@@ -455,6 +478,7 @@ hs_status hs_batch_info(hs_batch* b, int slot, hs_batch_inst_info* out) {
     out->applies32 = st.applies32; out->applies64 = st.applies64;
     out->rel_residual = st.rel64; out->d1_max64 = st.d1_max64; out->d1_max32 = st.d1_max32;
     out->tiles = sl.part.ntiles;
+    out->fault_fired = st.fi_fired; out->stalls = st.stalls; out->inner_faults = st.inner_faults;
     return HS_OK;
 }
 

@@ -23,7 +23,24 @@ struct BState {
     int outer, odone, pad1, pad2;
     // counters over the run
     long long inner_total, outer_total, applies32, applies64;
+    // armed vector fault of the current step: level 5 p32 (after formation),
+    // 6 r32 (after its update), 7 Ap32 (after projection), at correction
+    // fi_outer (1-based) and inner iteration fi_iter; 0 = none
+    int fi_vec, fi_outer, fi_iter, fi_bit;
+    long long fi_idx;
+    int fi_fired;           // the armed fault has fired
+    int stalls;             // steps that ended at max_outer without reaching rtol
+    int inner_bad;          // the current inner solve went non-finite: its correction is discarded
+    int inner_faults;       // inner solves discarded so far
 };
+
+__device__ __forceinline__ float flipf(float x, int bit) {
+    return __uint_as_float(__float_as_uint(x) ^ (1u << bit));
+}
+// the armed fault of level `vec` fires in this inner iteration
+__device__ __forceinline__ bool fi_now(const BState* st, int vec) {
+    return st->fi_vec == vec && st->outer == st->fi_outer && st->iter == st->fi_iter;
+}
 
 // instance descriptor (device array, rewritten by the host between rounds)
 struct BInst {
@@ -183,9 +200,25 @@ __global__ void __launch_bounds__(ST, 2) kb_apply(BatchArgs B) {
             rb[k] = (v && two) ? src_b[base + G.noff[k]] : (V)0;
         }
     };
-    auto form = [&](V (&p)[SK]) {
+    int fi_p = 0, fi_ap = 0, fi_bit = 0;
+    long long fi_idx = -1;
+    if constexpr (KIND == BK_LOOP) {
+        fi_p = fi_now(st, FI_P); fi_ap = fi_now(st, FI_AP);
+        fi_bit = st->fi_bit; fi_idx = st->fi_idx;
+    }
+    auto form = [&](V (&p)[SK], int px) {
 #pragma unroll
         for (int k = 0; k < SK; ++k) p[k] = two ? VT::fma(beta, rb[k], ra[k]) : ra[k];
+        if constexpr (KIND == BK_LOOP) {
+            if (fi_p) {
+#pragma unroll
+                for (int k = 0; k < SK; ++k)
+                    if (sp_valid(fl, k) && (long long)px * plane + G.noff[k] == fi_idx) {
+                        p[k] = flipf(p[k], fi_bit);
+                        st->fi_fired = 1;
+                    }
+            }
+        }
     };
     auto ld_coef = [&](int ex) {
         const bool ev = ex >= 0 && ex < N;
@@ -210,7 +243,7 @@ __global__ void __launch_bounds__(ST, 2) kb_apply(BatchArgs B) {
     };
     auto layer = [&](int ix, int cur, V (&pc)[SK], V (&pn)[SK], V (&ac)[SK], V (&an)[SK]) {
         const int nxt = cur ^ 1;
-        form(pn);
+        form(pn, ix + 1);
 #pragma unroll
         for (int k = 0; k < SK; ++k) S.P[nxt][tid + k * ST] = pn[k];
         ld_raw(ix + 2 <= xb + 1 ? ix + 2 : -2);
@@ -251,7 +284,10 @@ __global__ void __launch_bounds__(ST, 2) kb_apply(BatchArgs B) {
             if (ix >= xa) {
                 const long long n = base + G.noff[k];
                 const bool bnd = !yzin || xbnd;
-                const V y = bnd ? (V)0 : VT::add(VT::add(VT::add(ac[k], y3.x), y2.x), y1.x);
+                V y = bnd ? (V)0 : VT::add(VT::add(VT::add(ac[k], y3.x), y2.x), y1.x);
+                if constexpr (KIND == BK_LOOP) {
+                    if (fi_ap && n == fi_idx) { y = flipf(y, fi_bit); st->fi_fired = 1; }
+                }
                 const double pv = (double)pc[k], yd = (double)y;
                 if (loop) part[0] = dfma(pv, yd, part[0]);
                 if (d1) {
@@ -267,7 +303,7 @@ __global__ void __launch_bounds__(ST, 2) kb_apply(BatchArgs B) {
         ld_w(ix + 1);
     };
     ld_raw(xa - 1);
-    form(pA);
+    form(pA, xa - 1);
 #pragma unroll
     for (int k = 0; k < SK; ++k) { S.P[0][tid + k * ST] = pA[k]; aA[k] = (V)0; aB[k] = (V)0; }
     ld_raw(xa);
@@ -339,7 +375,8 @@ __global__ void __launch_bounds__(RT) kb_final_apply(BatchArgs B) {
     }
     if (KIND == BK_LOOP) {
         st->applies32 += 1;
-        if (fabs(p[0]) < 1e-30) { st->broken = 1; st->done = 1; }
+        if (!isfinite(p[0])) { st->inner_bad = 1; st->done = 1; }
+        else if (fabs(p[0]) < 1e-30) { st->broken = 1; st->done = 1; }
         else st->alpha = __ddiv_rn(st->rho, p[0]);
     } else {
         st->applies64 += 1;
@@ -412,16 +449,21 @@ __global__ void __launch_bounds__(RT) kb_outer_final(BatchArgs B) {
         st->bn64 = bn;
     }
     st->rel64 = __ddiv_rn(__dsqrt_rn(p[0]), st->bn64);
-    const bool conv = st->rel64 < B.rtol || !(st->rel64 == st->rel64);
-    if (conv || st->outer >= B.max_outer) { st->odone = 1; st->done = 1; return; }
+    const bool conv = st->rel64 < B.rtol;
+    if (conv || st->outer >= B.max_outer) {
+        if (!conv) st->stalls += 1;
+        st->odone = 1; st->done = 1;
+        return;
+    }
     st->outer += 1;
     st->outer_total += 1;
     st->rho = p[2];
     st->bn_in = __dsqrt_rn(p[3]);
     // solve only as far as the outer target needs: max(inner_tol, rtol / (2 rel64))
     st->tol_in = fmax(B.inner_tol, __ddiv_rn(0.5 * B.rtol, st->rel64));
-    st->iter = 0; st->broken = 0; st->beta = 0.0;
-    st->done = (st->bn_in < 1e-300) ? 1 : 0;
+    st->iter = 0; st->broken = 0; st->beta = 0.0; st->inner_bad = 0;
+    st->done = (st->bn_in < 1e-300 || !isfinite(st->bn_in) || !isfinite(p[2])) ? 1 : 0;
+    if (!isfinite(st->bn_in) || !isfinite(p[2])) st->inner_bad = 1;
 }
 
 // inner FP32 update: d += alpha p, r -= alpha Ap, z = r / diag; partials r.r, r.z
@@ -436,10 +478,12 @@ __global__ void __launch_bounds__(RT) kb_update32(BatchArgs B) {
             const int iter = st->iter;
             const float alpha = (float)st->alpha;
             const float* p = (iter & 1) ? I.p32b : I.p32a;
+            const bool fr = fi_now(st, FI_RV);
             for (int k = 0; k < f.cnt; ++k) {
                 const long long m = f.m0 + k;
                 I.d32[m] = __fmaf_rn(alpha, p[m], I.d32[m]);
-                const float r = __fmaf_rn(-alpha, I.Ap32[m], I.r32[m]);
+                float r = __fmaf_rn(-alpha, I.Ap32[m], I.r32[m]);
+                if (fr && m == st->fi_idx) { r = flipf(r, st->fi_bit); I.st->fi_fired = 1; }
                 const float z = __fmul_rn(r, I.dinv32[m]);
                 I.r32[m] = r; I.z32[m] = z;
                 part[0] = dfma((double)r, (double)r, part[0]);
@@ -465,22 +509,35 @@ __global__ void __launch_bounds__(RT) kb_final_update32(BatchArgs B) {
     if (threadIdx.x != 0) return;
     st->inner_total += 1;
     const double rel = __ddiv_rn(__dsqrt_rn(p[0]), st->bn_in);
-    if (rel < st->tol_in || !(rel == rel) || st->iter + 1 >= B.max_inner) { st->done = 1; return; }
+    if (!isfinite(rel) || !isfinite(p[1])) { st->inner_bad = 1; st->done = 1; return; }
+    if (rel < st->tol_in || st->iter + 1 >= B.max_inner) { st->done = 1; return; }
     st->beta = __ddiv_rn(p[1], st->rho);
     st->rho = p[1];
     st->iter += 1;
 }
 
-// T += d (FP64) for the instances whose inner solve just finished
+// T += d (FP64) at the interior nodes, for the instances whose inner solve
+// just finished; Dirichlet values are never changed, and a correction from an
+// inner solve that went non-finite is discarded (the next correction re-solves)
 __global__ void __launch_bounds__(RT) kb_correct(BatchArgs B) {
     const FlatPos f = flat_pos(B);
     if (f.slot < 0) return;
     const BInst& I = B.inst[f.slot];
-    if (!I.active || I.st->odone) return;
+    if (!I.active || I.st->odone || I.st->inner_bad) return;
+    const int N = I.part.N;
     for (int k = 0; k < f.cnt; ++k) {
         const long long m = f.m0 + k;
-        I.T[m] = dadd(I.T[m], (double)I.d32[m]);
+        if (!is_bnd(m, N)) I.T[m] = dadd(I.T[m], (double)I.d32[m]);
     }
+}
+
+// count the discarded inner solves (one thread per instance, after kb_correct)
+__global__ void kb_count_bad(BatchArgs B) {
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= B.n_inst) return;
+    const BInst& I = B.inst[slot];
+    if (!I.active || I.st->odone) return;
+    if (I.st->inner_bad) I.st->inner_faults += 1;
 }
 
 // set-up helpers: FP32 reciprocal of the diagonal; the interior indicator
@@ -492,6 +549,11 @@ __global__ void k_ones_interior(int N, double* v) {
     const long long NN = N + 1, Nn = NN * NN * NN;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < Nn; i += (long long)gridDim.x * blockDim.x)
         v[i] = is_bnd(i, N) ? 0.0 : 1.0;
+}
+
+// arm (vec > 0) or disarm (vec == 0) the vector fault of one instance
+__global__ void kb_arm(BState* st, int vec, int outer, int iter, long long idx, int bit) {
+    st->fi_vec = vec; st->fi_outer = outer; st->fi_iter = iter; st->fi_idx = idx; st->fi_bit = bit;
 }
 
 // step start: outer state of every active instance

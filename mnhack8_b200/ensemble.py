@@ -12,6 +12,9 @@ GPU and the same seeded synthetic inputs, and prints one JSON line.
              16..96, lognormal k sigma 1 with correlation N/8 elements),
              20 steps each to rtol 1e-8, all in one batch (one graph launch
              per step); the tile depth is chosen by a short autotuning run.
+  coverage   detection coverage of the mixed form under 1000 seeded flips
+             into its FP32 inner vectors, beside the FP64 drop-in's campaign
+             (p, r, Ap) on the same problem (N=64 by default).
   serving    a seeded Poisson stream of requests (N uniform in 16..160, steps
              uniform in 10..100, 30 % with one seeded bit flip of the field),
              served by continuous batching: requests join the running batch
@@ -274,6 +277,103 @@ def serving(n=400, rate=200.0, seed=11, rtol=1e-8, inner_tol=1e-4, max_live=64, 
     }
 
 
+# ---- config 3: detection coverage of the mixed form, beside FP64 ------------------------
+def coverage(N=64, steps=20, flips=1000, seed=21, per_batch=125, rtol=1e-8, inner_tol=1e-4, sigma=1.5,
+             corr_frac=1.0 / 16.0, sig_err=1e-6, device=0, rows_out=None, fp64=True):
+    """Seeded single-bit flips into the FP32 inner vectors of the mixed form
+    (p after formation, r after its update, Ap after projection; bits 0..31,
+    step and inner iteration of the first correction uniform), run as batches
+    of faulted copies of one problem, beside the FP64 drop-in's campaign
+    (p, r, Ap, bits 0..63) on the same problem.  A mixed-form flip counts as
+    detected when an FP32 apply's D1 exceeds 100x the clean run's FP32 noise
+    floor, an FP64 apply's D1 exceeds 1e-10, or a step ends at the correction
+    cap or an inner solve goes non-finite (its correction is then discarded);
+    it is significant when its final field error exceeds sig_err (or is not
+    finite)."""
+    from mnhack8_b200.campaign import coverage as fp64_coverage
+    (k, r), = lognormal_many([(N, sigma, corr_frac * N, 3)], workers=1)
+    T0 = _lib.gaussian_ic(N, IC_SIGMA)
+    Nn = (N + 1) ** 3
+    b = _lib.Batch(rtol=rtol, inner_tol=inner_tol, device=device)
+    s = b.add(N, DT, k, r, T0=T0, steps=steps)
+    while b.step()[0]:
+        pass
+    T_clean, clean = b.field(s), b.info(s)
+    b.close()
+    thr32 = max(100.0 * clean["d1_max32"], 1e-12)
+    per_corr = max(1, int(clean["inner_iters"] / max(1, clean["outer_iters"])))
+    rng = np.random.default_rng(seed)
+    sites = [dict(level=int(rng.choice([5, 6, 7])), step=int(rng.integers(0, steps)), outer=1,
+                  iter=int(rng.integers(0, per_corr)), idx=int(rng.integers(0, Nn)), bit=int(rng.integers(0, 32)))
+             for _ in range(flips)]
+    t0 = time.perf_counter()
+    rows = []
+    for c0 in range(0, flips, per_batch):
+        chunk = sites[c0:c0 + per_batch]
+        b = _lib.Batch(rtol=rtol, inner_tol=inner_tol, device=device)
+        slots = []
+        for f in chunk:
+            sl = b.add(N, DT, k, r, T0=T0, steps=steps)
+            b.arm_fault(sl, f["level"], f["step"], f["outer"], f["iter"], f["idx"], f["bit"])
+            slots.append(sl)
+        while b.step()[0]:
+            pass
+        for f, sl in zip(chunk, slots):
+            inf = b.info(sl)
+            T = b.field(sl)
+            err = float(np.linalg.norm(T - T_clean) / np.linalg.norm(T_clean)) if np.all(np.isfinite(T)) \
+                else float("inf")
+            det = (inf["d1_max32"] > thr32 or inf["d1_max64"] > 1e-10 or inf["stalls"] > 0 or
+                   inf["inner_faults"] > 0)
+            rows.append(dict(f, fired=inf["fault_fired"], err=err, detected=bool(det), stalls=inf["stalls"],
+                             inner_faults=inf["inner_faults"],
+                             d1_max32=inf["d1_max32"], extra_inner=inf["inner_iters"] - clean["inner_iters"]))
+        b.close()
+    wall = time.perf_counter() - t0
+    fired = [x for x in rows if x["fired"]]
+    sig = [x for x in fired if not (x["err"] <= sig_err)]
+
+    def share(sel, pool):
+        return (sum(1 for x in pool if sel(x)) / len(pool)) if pool else None
+
+    mixed = {
+        "flips": flips, "fired": len(fired), "significant": len(sig),
+        "detected_rate_of_fired": share(lambda x: x["detected"], fired),
+        "coverage_of_significant": share(lambda x: x["detected"], sig),
+        "missed_significant": sum(1 for x in sig if not x["detected"]),
+        "silent_corruptions": sum(1 for x in sig if not x["detected"]),
+        "abft_d1_rate_of_fired": share(lambda x: x["d1_max32"] > thr32, fired),
+        "max_err_of_undetected": max([x["err"] for x in fired if not x["detected"]] or [0.0]),
+        "median_extra_inner_iters": float(np.median([x["extra_inner"] for x in fired])) if fired else None,
+        "fp32_noise_floor_max_d1": clean["d1_max32"], "fp32_threshold": thr32, "wall_s": wall,
+        "by_vector": {v: {"fired": sum(1 for x in fired if x["level"] == lv),
+                          "detected_rate": share(lambda x: x["detected"], [x for x in fired if x["level"] == lv])}
+                      for v, lv in (("p", 5), ("r", 6), ("Ap", 7))},
+    }
+    if rows_out:
+        with open(rows_out, "w") as fh:
+            json.dump(rows, fh, default=lambda v: None if isinstance(v, float) and not np.isfinite(v) else v)
+    if not fp64:
+        return {"form": "precision-coverage", "N": N, "mixed": mixed}
+    # FP64 drop-in: the same problem through hs_campaign
+    g = _lib.Solver(N, DT, k, r, kernel="wht", scatter="colored", detect=True, no_source=True, ic="gaussian",
+                    ic_sigma=IC_SIGMA, rtol=rtol, max_iter=1000, device=device)
+    t0 = time.perf_counter()
+    clean64, recs = g.campaign(steps, 1, flips, seed)
+    wall64 = time.perf_counter() - t0
+    g.close()
+    cov64 = fp64_coverage(recs, clean64, sig_err)
+    fp64 = {k2: cov64[k2] for k2 in ("flips", "significant", "any_detector_coverage_of_significant",
+                                      "missed_significant", "abft_d1_rate", "any_detector_rate",
+                                      "abft_noise_floor_clean_max_d1")}
+    fp64["wall_s"] = wall64
+    fp64["silent_corruptions"] = cov64["missed_significant"]
+    return {"form": "precision-coverage", "N": N, "steps": steps, "rtol": rtol, "significant_error": sig_err,
+            "mixed": mixed, "fp64": fp64,
+            "abft_d1_rate_difference_points": 100.0 * (mixed["abft_d1_rate_of_fired"] - fp64["abft_d1_rate"]),
+            "silent_corruptions": {"mixed": mixed["silent_corruptions"], "fp64": fp64["silent_corruptions"]}}
+
+
 def _main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -284,6 +384,11 @@ def _main(argv=None):
     p.add_argument("--n", type=int, default=256)
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--serial-sample", type=int, default=None)
+    p = sub.add_parser("coverage")
+    p.add_argument("--N", type=int, default=64)
+    p.add_argument("--flips", type=int, default=1000)
+    p.add_argument("--rows", default=None, help="write the mixed form's per-flip rows (JSON) here")
+    p.add_argument("--no-fp64", action="store_true")
     p = sub.add_parser("serving")
     p.add_argument("--n", type=int, default=400)
     p.add_argument("--rate", type=float, default=200.0)
@@ -291,6 +396,8 @@ def _main(argv=None):
     a = ap.parse_args(argv)
     if a.cmd == "precision":
         out = precision(N=a.N, steps=a.steps)
+    elif a.cmd == "coverage":
+        out = coverage(N=a.N, flips=a.flips, rows_out=a.rows, fp64=not a.no_fp64)
     elif a.cmd == "batching":
         out = batching(n=a.n, steps=a.steps, serial_sample=a.serial_sample)
     else:

@@ -108,3 +108,56 @@ def test_bad_arguments():
         b.remove(3)
     assert b.step() == (0, 0.0)
     b.close()
+
+
+def test_inner_fault_fires_is_detected_and_corrected(oracle):
+    """A flip in an FP32 inner vector fires once, an exponent flip of Ap
+    shows in the FP32 checksum, and the FP64 defect correction still brings
+    the step to the clean answer; a site past the inner solve never fires."""
+    N, dt, steps = 12, 5e-4, 3
+    k, r = field(N, "lognormal", sigma=1.0, L=0.25, seed=9)
+    T0 = gaussian_T0(oracle, N, dt, k, r)
+    b = _lib.Batch(rtol=1e-8)
+    clean = b.add(N, dt, k, r, T0=T0, steps=steps)
+    hit = b.add(N, dt, k, r, T0=T0, steps=steps)
+    miss = b.add(N, dt, k, r, T0=T0, steps=steps)
+    mid = 6 * 169 + 6 * 13 + 6
+    b.arm_fault(hit, "AP", 1, 1, 2, mid, 29)        # exponent bit of Ap32
+    b.arm_fault(miss, "P", 1, 1, 10000, mid, 29)    # iteration never reached
+    while b.step()[0]:
+        pass
+    c, h, m = b.info(clean), b.info(hit), b.info(miss)
+    assert h["fault_fired"] == 1 and m["fault_fired"] == 0 and c["fault_fired"] == 0
+    assert h["d1_max32"] > 1e3 * c["d1_max32"]
+    Tc, Th = b.field(clean), b.field(hit)
+    assert np.linalg.norm(Th - Tc) <= 1e-7 * np.linalg.norm(Tc)
+    assert h["rel_residual"] < 1e-8 and h["stalls"] == 0
+    assert np.array_equal(bits(b.field(miss)), bits(Tc))
+    b.close()
+
+
+def test_boundary_and_nonfinite_faults_heal(oracle):
+    """Flips the FP64 residual cannot see (a Dirichlet entry) or that make the
+    inner solve non-finite (an r exponent flip) leave the answer at the clean
+    one: corrections never touch Dirichlet nodes, and a non-finite inner solve
+    is discarded and solved again."""
+    N, dt, steps = 12, 5e-4, 3
+    k, r = field(N, "lognormal", sigma=1.0, L=0.25, seed=9)
+    T0 = gaussian_T0(oracle, N, dt, k, r)
+    b = _lib.Batch(rtol=1e-8)
+    clean = b.add(N, dt, k, r, T0=T0, steps=steps)
+    bnd = b.add(N, dt, k, r, T0=T0, steps=steps)
+    nf = b.add(N, dt, k, r, T0=T0, steps=steps)
+    b.arm_fault(bnd, "P", 1, 1, 3, 5, 30)                        # node 5 lies on the x = 0 face
+    b.arm_fault(nf, "RV", 1, 1, 3, 6 * 169 + 6 * 13 + 6, 30)     # r exponent flip: z overflows
+    while b.step()[0]:
+        pass
+    Tc = b.field(clean)
+    for s in (bnd, nf):
+        inf = b.info(s)
+        assert inf["fault_fired"] == 1 and inf["stalls"] == 0 and inf["rel_residual"] < 1e-8
+        T = b.field(s)
+        assert np.all(np.isfinite(T))
+        assert np.linalg.norm(T - Tc) <= 1e-7 * np.linalg.norm(Tc)
+    assert b.info(nf)["inner_faults"] >= 1
+    b.close()
