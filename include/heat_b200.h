@@ -246,7 +246,8 @@ typedef struct hs_batch_options {
     int max_outer;        /* corrections per step */
     int max_inner;        /* inner PCG iterations per correction */
     int detect;           /* ABFT checksum on every operator apply */
-    int tile_planes;      /* operator tiles span min(N+1, tile_planes) planes (0: 32) */
+    int tile_planes;      /* operator tiles span min(N+1, tile_planes) planes; 0: a depth set by N
+                             alone (the instance by itself fills the GPU, within 8..32 planes) */
     int device;
     int pad;
 } hs_batch_options;

@@ -397,7 +397,7 @@ class Batch:
     """Batched mixed-precision solves (hs_batch_*): instances added to slots
     advance one implicit-Euler step per step() call, all in one graph launch."""
 
-    def __init__(self, rtol=1e-8, inner_tol=1e-4, max_outer=10, max_inner=500, detect=True, tile_planes=32,
+    def __init__(self, rtol=1e-8, inner_tol=1e-4, max_outer=10, max_inner=500, detect=True, tile_planes=0,
                  device=0):
         o = BatchOptions()
         lib().hs_batch_default_options(C.byref(o))

@@ -21,8 +21,10 @@
 namespace {
 
 // tile shape of one batched instance: C, R as in the slab layout (largest
-// tile plane that fits, fewest positions loaded per node), CX = min(N+1,
-// planes) planes per tile
+// tile plane that fits, fewest positions loaded per node) and CX planes per
+// tile: min(N+1, planes), or with planes == 0 a function of N alone (the
+// depth at which the instance by itself fills SLAB_SLOTS tiles, within 8..32),
+// so that an instance's arithmetic never depends on the rest of the batch
 Part batch_part(int N, int planes) {
     const long long NN = N + 1;
     long long bestC = NN, bestR = 1, best_cost = -1;
@@ -36,8 +38,13 @@ Part batch_part(int N, int planes) {
         const long long cost = NCB * NRB * (Cw * (R + 2) + 2 * (C + 1) * (R + 1));
         if (best_cost < 0 || cost < best_cost) { best_cost = cost; bestC = C; bestR = R; }
     }
-    if (planes < 1) planes = 32;
-    const long long CX = planes < NN ? planes : NN;
+    const long long tyz = ((NN + bestC - 1) / bestC) * ((NN + bestR - 1) / bestR);
+    long long depth = planes;
+    if (planes < 1) {
+        depth = (NN * tyz + SLAB_SLOTS - 1) / SLAB_SLOTS;
+        depth = depth < 8 ? 8 : (depth > 32 ? 32 : depth);
+    }
+    const long long CX = depth < NN ? depth : NN;
     Part p{};
     p.N = N; p.NN = (int)NN;
     p.C = (int)bestC; p.R = (int)bestR; p.CX = (int)CX;
@@ -174,7 +181,7 @@ hs_status build_batch_graph(hs_batch* b) {
     kb_apply<double, BK_RHS><<<(int)a.ntiles, ST, sizeof(BSlabSmem<double>), b->s>>>(a);
     kb_final_apply<BK_RHS><<<a.n_inst, RT, 0, b->s>>>(a);
     enqueue_resid(b, a);
-    kb_cond<0><<<1, 1024, 0, b->s>>>(a, c_out);
+    kb_cond<0><<<1, 1024, 0, b->s>>>(a, c_out, nullptr);
     HS_CUDA(cudaStreamEndCapture(b->s, &pre));
     cudaGraphNode_t n_pre;
     HS_CUDA(cudaGraphAddChildGraphNode(&n_pre, g, nullptr, 0, pre));
@@ -191,7 +198,7 @@ hs_status build_batch_graph(hs_batch* b) {
     HS_CUDA(cudaGraphConditionalHandleCreate(&c_in, obody, 0, cudaGraphCondAssignDefault));
     cudaGraph_t ohead;
     HS_CUDA(cudaStreamBeginCapture(b->s, cudaStreamCaptureModeThreadLocal));
-    kb_cond<1><<<1, 1024, 0, b->s>>>(a, c_in);
+    kb_cond<1><<<1, 1024, 0, b->s>>>(a, c_in, nullptr);
     HS_CUDA(cudaStreamEndCapture(b->s, &ohead));
     cudaGraphNode_t n_head;
     HS_CUDA(cudaGraphAddChildGraphNode(&n_head, obody, nullptr, 0, ohead));
@@ -209,20 +216,60 @@ hs_status build_batch_graph(hs_batch* b) {
     kb_final_apply<BK_LOOP><<<a.n_inst, RT, 0, b->s>>>(a);
     kb_update32<<<(int)a.nflat, RT, 0, b->s>>>(a);
     kb_final_update32<<<a.n_inst, RT, 0, b->s>>>(a);
-    kb_cond<1><<<1, 1024, 0, b->s>>>(a, c_in);
+    kb_cond<1><<<1, 1024, 0, b->s>>>(a, c_in, nullptr);
     HS_CUDA(cudaStreamEndCapture(b->s, &ibody));
     cudaGraph_t otail;
     HS_CUDA(cudaStreamBeginCapture(b->s, cudaStreamCaptureModeThreadLocal));
     kb_correct<<<(int)a.nflat, RT, 0, b->s>>>(a);
     kb_count_bad<<<(a.n_inst + 127) / 128, 128, 0, b->s>>>(a);
     enqueue_resid(b, a);
-    kb_cond<0><<<1, 1024, 0, b->s>>>(a, c_out);
+    kb_cond<0><<<1, 1024, 0, b->s>>>(a, c_out, nullptr);
     HS_CUDA(cudaStreamEndCapture(b->s, &otail));
     cudaGraphNode_t n_tail;
     HS_CUDA(cudaGraphAddChildGraphNode(&n_tail, obody, &n_in, 1, otail));
     cudaGraphDestroy(otail);
     HS_CUDA(cudaGraphInstantiate(&b->gexec, g, 0));
     b->graph = g;
+    return HS_OK;
+}
+
+// One step as direct launches with the loop conditions read back by the host
+// (HS_GRAPH=0: profilers cannot attribute kernels inside conditional nodes).
+// Both loops stay bounded by max_outer / max_inner through the same flags.
+hs_status step_direct(hs_batch* b) {
+    const BatchArgs a = batch_args(b);
+    DevBuf<int> flag;
+    HS_CUDA(flag.alloc(2));
+    int host_flag = 0;
+    auto read = [&](int i) -> hs_status {
+        HS_CUDA(cudaMemcpyAsync(&host_flag, flag.p + i, sizeof(int), cudaMemcpyDeviceToHost, b->s));
+        HS_CUDA(cudaStreamSynchronize(b->s));
+        return HS_OK;
+    };
+    kb_step_begin<<<(a.n_inst + 127) / 128, 128, 0, b->s>>>(a);
+    kb_apply<double, BK_RHS><<<(int)a.ntiles, ST, sizeof(BSlabSmem<double>), b->s>>>(a);
+    kb_final_apply<BK_RHS><<<a.n_inst, RT, 0, b->s>>>(a);
+    enqueue_resid(b, a);
+    kb_cond<0><<<1, 1024, 0, b->s>>>(a, 0, flag.p);
+    for (;;) {
+        if (read(0) != HS_OK) return HS_ERR_CUDA;
+        if (!host_flag) break;
+        kb_cond<1><<<1, 1024, 0, b->s>>>(a, 0, flag.p + 1);
+        for (;;) {
+            if (read(1) != HS_OK) return HS_ERR_CUDA;
+            if (!host_flag) break;
+            kb_apply<float, BK_LOOP><<<(int)a.ntiles, ST, sizeof(BSlabSmem<float>), b->s>>>(a);
+            kb_final_apply<BK_LOOP><<<a.n_inst, RT, 0, b->s>>>(a);
+            kb_update32<<<(int)a.nflat, RT, 0, b->s>>>(a);
+            kb_final_update32<<<a.n_inst, RT, 0, b->s>>>(a);
+            kb_cond<1><<<1, 1024, 0, b->s>>>(a, 0, flag.p + 1);
+        }
+        kb_correct<<<(int)a.nflat, RT, 0, b->s>>>(a);
+        kb_count_bad<<<(a.n_inst + 127) / 128, 128, 0, b->s>>>(a);
+        enqueue_resid(b, a);
+        kb_cond<0><<<1, 1024, 0, b->s>>>(a, 0, flag.p);
+    }
+    HS_CUDA(cudaGetLastError());
     return HS_OK;
 }
 
@@ -234,7 +281,7 @@ void hs_batch_default_options(hs_batch_options* o) {
     if (!o) return;
     std::memset(o, 0, sizeof(*o));
     o->rtol = 1e-8; o->inner_tol = 1e-4; o->max_outer = 10; o->max_inner = 500;
-    o->detect = 1; o->tile_planes = 32; o->device = 0;
+    o->detect = 1; o->tile_planes = 0; o->device = 0;
 }
 
 hs_status hs_batch_create(const hs_batch_options* opt, hs_batch** out) {
@@ -432,7 +479,8 @@ hs_status hs_batch_step(hs_batch* b, int* n_active, double* device_ms) {
         if (st != HS_OK) return st;
         for (auto& sl : b->slots) sl.desc.active = (sl.used && sl.steps_left > 0) ? 1 : 0;
     }
-    hs_status st = build_batch_graph(b);
+    const bool graph = graphs_enabled();
+    hs_status st = graph ? build_batch_graph(b) : HS_OK;
     if (st != HS_OK) return st;
     // armed flips of this step (level G: one bit of the field before the step)
     for (auto& sl : b->slots) {
@@ -446,7 +494,12 @@ hs_status hs_batch_step(hs_batch* b, int* n_active, double* device_ms) {
     HS_CUDA(cudaEventCreate(&e0));
     HS_CUDA(cudaEventCreate(&e1));
     HS_CUDA(cudaEventRecord(e0, b->s));
-    HS_CUDA(cudaGraphLaunch(b->gexec, b->s));
+    if (graph) {
+        HS_CUDA(cudaGraphLaunch(b->gexec, b->s));
+    } else {
+        st = step_direct(b);
+        if (st != HS_OK) return st;
+    }
     HS_CUDA(cudaEventRecord(e1, b->s));
     HS_CUDA(cudaEventSynchronize(e1));
     HS_CUDA(cudaGetLastError());

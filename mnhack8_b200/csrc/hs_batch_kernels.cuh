@@ -569,7 +569,7 @@ __global__ void kb_step_begin(BatchArgs B) {
 // loop conditions: any active instance still in its outer loop (WHICH 0) /
 // in an inner solve (WHICH 1)
 template <int WHICH>
-__global__ void kb_cond(BatchArgs B, cudaGraphConditionalHandle h) {
+__global__ void kb_cond(BatchArgs B, cudaGraphConditionalHandle h, int* flag) {
     int any = 0;
     for (int s = threadIdx.x; s < B.n_inst; s += blockDim.x) {
         const BInst& I = B.inst[s];
@@ -578,7 +578,10 @@ __global__ void kb_cond(BatchArgs B, cudaGraphConditionalHandle h) {
         if (WHICH == 0 ? !st->odone : (!st->odone && !st->done)) any = 1;
     }
     any = __syncthreads_or(any);
-    if (threadIdx.x == 0) cudaGraphSetConditional(h, any ? 1u : 0u);
+    if (threadIdx.x == 0) {
+        if (flag) *flag = any;                      // direct launches: the host reads the flag
+        else cudaGraphSetConditional(h, any ? 1u : 0u);
+    }
 }
 
 }  // namespace hs

@@ -42,7 +42,7 @@ def test_mixed_precision_reaches_fp64(oracle):
 CASES = [(8, 1e-3, 4, 1), (13, 5e-4, 6, 2), (20, 2e-4, 3, 3), (5, 2e-3, 5, 4)]
 
 
-def _solo(oracle, N, dt, steps, seed, planes=32):
+def _solo(oracle, N, dt, steps, seed, planes=0):
     k, r = field(N, "lognormal", sigma=1.0, L=0.25, seed=seed)
     b = _lib.Batch(rtol=1e-8, tile_planes=planes)
     s = b.add(N, dt, k, r, T0=gaussian_T0(oracle, N, dt, k, r), steps=steps)
@@ -95,7 +95,7 @@ def test_join_running_batch_and_reuse_slot(oracle):
 
 
 def test_tile_depth_changes_only_rounding(oracle):
-    T1, _ = _solo(oracle, 20, 2e-4, 3, 3, planes=32)
+    T1, _ = _solo(oracle, 20, 2e-4, 3, 3, planes=0)
     T4, _ = _solo(oracle, 20, 2e-4, 3, 3, planes=5)
     assert np.linalg.norm(T1 - T4) <= 1e-7 * np.linalg.norm(T1)
 
@@ -161,3 +161,39 @@ def test_boundary_and_nonfinite_faults_heal(oracle):
         assert np.linalg.norm(T - Tc) <= 1e-7 * np.linalg.norm(Tc)
     assert b.info(nf)["inner_faults"] >= 1
     b.close()
+
+
+_DIRECT = r"""
+import sys, hashlib
+sys.path.insert(0, {root!r})
+import numpy as np
+from mnhack8_b200 import _lib
+from tests.helpers import field
+k, r = field(10, "lognormal", sigma=1.0, L=0.25, seed=6)
+b = _lib.Batch(rtol=1e-8)
+s = b.add(10, 1e-3, k, r, T0=_lib.gaussian_ic(10, 0.15), steps=3)
+while b.step()[0]:
+    pass
+print(hashlib.sha256(b.field(s).tobytes()).hexdigest(), b.info(s)["inner_iters"])
+"""
+
+
+def test_direct_launches_equal_graph():
+    """HS_GRAPH=0 (direct launches, for profilers) computes the same bits as the graph."""
+    import hashlib
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    k, r = field(10, "lognormal", sigma=1.0, L=0.25, seed=6)
+    b = _lib.Batch(rtol=1e-8)
+    s = b.add(10, 1e-3, k, r, T0=_lib.gaussian_ic(10, 0.15), steps=3)
+    while b.step()[0]:
+        pass
+    want = f"{hashlib.sha256(b.field(s).tobytes()).hexdigest()} {b.info(s)['inner_iters']}"
+    b.close()
+    env = dict(os.environ, HS_GRAPH="0")
+    out = subprocess.run([sys.executable, "-c", _DIRECT.format(root=root)], env=env, capture_output=True,
+                         text=True, timeout=300, cwd=root)
+    assert out.returncode == 0, out.stderr[-2000:]
+    assert out.stdout.strip().splitlines()[-1] == want
