@@ -564,10 +564,12 @@ struct UpdateArgs {
     int use_cond, pad;
 };
 
-// PCG vector update on the flat partition: each thread updates its KF = 2
-// consecutive nodes (128-bit loads and stores), in order.
-__global__ void __launch_bounds__(RT, 6) k_update(UpdateArgs a) {
-    static_assert(KF == 2, "two nodes per thread");
+// PCG vector update on the flat partition: each thread updates its KF
+// consecutive nodes (KF / 2 aligned 128-bit loads and stores per vector), in
+// order.
+__global__ void __launch_bounds__(RT, KF <= 2 ? 6 : (KF <= 4 ? 4 : 2)) k_update(UpdateArgs a) {
+    static_assert(KF % 2 == 0, "pairs of nodes per thread");
+    constexpr int NC = KF / 2;
     __shared__ double sh[MAXQ][8];
     DevState* st = a.st;
     const int tid = threadIdx.x;
@@ -586,46 +588,58 @@ __global__ void __launch_bounds__(RT, 6) k_update(UpdateArgs a) {
     const double nalpha = -alpha;
     double part[3] = {0.0, 0.0, 0.0};   // PRE: bb, rz, rr   LOOP: rr, rz, -
     const long long m0 = ((long long)blockIdx.x * RT + tid) * KF;
-    const int cnt = (m0 + 1 < a.Nn) ? 2 : (m0 < a.Nn ? 1 : 0);
-    auto ld2 = [&](const double* base, double& u, double& v) {
-        if (cnt == 2) { const double2 t = __ldg(reinterpret_cast<const double2*>(base + m0)); u = t.x; v = t.y; }
-        else { u = cnt ? __ldg(base + m0) : 0.0; v = 0.0; }
-    };
-    auto st2 = [&](double* base, double u, double v) {
-        if (cnt == 2) *reinterpret_cast<double2*>(base + m0) = make_double2(u, v);
-        else if (cnt == 1) base[m0] = u;
-    };
-    if (pre) {
-        double b0, b1, q0, q1, d0, d1;
-        ld2(a.b, b0, b1); ld2(a.Ap, q0, q1); ld2(a.d, d0, d1);
-        double r_[2], z_[2];
-        const double bb[2] = {b0, b1}, qq[2] = {q0, q1}, dd[2] = {d0, d1};
+    int cnt[NC];
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            if (k >= cnt) break;
+    for (int c = 0; c < NC; ++c) {
+        const long long m = m0 + 2 * c;
+        cnt[c] = (m + 1 < a.Nn) ? 2 : (m < a.Nn ? 1 : 0);
+    }
+    auto ld = [&](const double* base, double (&v)[KF]) {
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            const long long m = m0 + 2 * c;
+            if (cnt[c] == 2) { const double2 t = __ldg(reinterpret_cast<const double2*>(base + m)); v[2 * c] = t.x; v[2 * c + 1] = t.y; }
+            else { v[2 * c] = cnt[c] ? __ldg(base + m) : 0.0; v[2 * c + 1] = 0.0; }
+        }
+    };
+    auto stv = [&](double* base, const double (&v)[KF]) {
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            const long long m = m0 + 2 * c;
+            if (cnt[c] == 2) *reinterpret_cast<double2*>(base + m) = make_double2(v[2 * c], v[2 * c + 1]);
+            else if (cnt[c] == 1) base[m] = v[2 * c];
+        }
+    };
+    auto has = [&](int k) { return k % 2 < cnt[k / 2]; };
+    if (pre) {
+        double bb[KF], qq[KF], dd[KF], r_[KF], z_[KF];
+        ld(a.b, bb); ld(a.Ap, qq); ld(a.d, dd);
+#pragma unroll
+        for (int k = 0; k < KF; ++k) {
+            r_[k] = 0.0; z_[k] = 0.0;
+            if (!has(k)) continue;
             r_[k] = dfma(-1.0, qq[k], bb[k]);
             z_[k] = __ddiv_rn(r_[k], dd[k]);
             part[0] = dfma(bb[k], bb[k], part[0]);
             part[1] = dfma(r_[k], z_[k], part[1]);
             part[2] = dfma(r_[k], r_[k], part[2]);
         }
-        st2(a.r, r_[0], r_[1]); st2(a.z, z_[0], z_[1]);
+        stv(a.r, r_); stv(a.z, z_);
     } else {
-        double x0, x1, p0, p1, q0, q1, r0, r1, d0, d1;
-        ld2(a.x, x0, x1); ld2(p, p0, p1); ld2(a.Ap, q0, q1); ld2(a.r, r0, r1); ld2(a.d, d0, d1);
-        const double xx[2] = {x0, x1}, pp[2] = {p0, p1}, qq[2] = {q0, q1}, rr[2] = {r0, r1}, dd[2] = {d0, d1};
-        double xn[2], r_[2], z_[2];
+        double xx[KF], pp[KF], qq[KF], rr[KF], dd[KF];
+        ld(a.x, xx); ld(p, pp); ld(a.Ap, qq); ld(a.r, rr); ld(a.d, dd);
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            if (k >= cnt) break;
-            xn[k] = dfma(alpha, pp[k], xx[k]);
-            r_[k] = dfma(nalpha, qq[k], rr[k]);
-            if (fi_r && m0 + k == fi_idx) r_[k] = flipbit(r_[k], fi_bit);
-            z_[k] = __ddiv_rn(r_[k], dd[k]);
-            part[0] = dfma(r_[k], r_[k], part[0]);
-            part[1] = dfma(r_[k], z_[k], part[1]);
+        for (int k = 0; k < KF; ++k) {
+            if (!has(k)) continue;
+            xx[k] = dfma(alpha, pp[k], xx[k]);
+            double rk = dfma(nalpha, qq[k], rr[k]);
+            if (fi_r && m0 + k == fi_idx) rk = flipbit(rk, fi_bit);
+            rr[k] = rk;
+            dd[k] = __ddiv_rn(rk, dd[k]);          // z
+            part[0] = dfma(rk, rk, part[0]);
+            part[1] = dfma(rk, dd[k], part[1]);
         }
-        st2(a.x, xn[0], xn[1]); st2(a.r, r_[0], r_[1]); st2(a.z, z_[0], z_[1]);
+        stv(a.x, xx); stv(a.r, rr); stv(a.z, dd);
     }
     store_partials<3>(part, a.partials, a.nflat, sh);
 }

@@ -28,7 +28,7 @@ namespace hs {
 // (the lower x layer first, each layer's own-column element first), skipping
 // elements outside the domain.
 constexpr int RT = 256;
-constexpr int KF = 2;
+constexpr int KF = 2;                 // nodes per thread of the flat partition
 constexpr int ST = RT;                // threads per slab CTA
 constexpr int SK = 4;                 // positions per thread
 constexpr int SPOS = ST * SK;         // positions per plane of a slab CTA (halo included)
