@@ -62,6 +62,8 @@ def parse():
     ap.add_argument("--no-detect", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-gate", action="store_true",
+                    help="skip the supplementary N=256 operator-kernel measurement")
     ap.add_argument("--profile", action="store_true",
                     help="only the timed trajectories (no e2e, kernel timing or CPU baseline): for ncu captures")
     return ap.parse_args()
@@ -341,6 +343,8 @@ def main():
         "gpu_launches": launches,
         "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"]},
     }
+    if rank == 0 and not args.no_gate and N != GATE_N:
+        line["apply_gate_N256"] = gate_apply(local, detect, args.kernel, args.scatter)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(N, args.cpu_seconds)
     if rank == 0:
@@ -350,6 +354,29 @@ def main():
         dist.barrier(device_ids=[local])
         dist.destroy_process_group()
     return 0
+
+
+GATE_N = 256
+
+
+def gate_apply(device, detect, kernel, scatter):
+    """Supplementary: the PCG operator kernel alone at N=256 (129^3 -> 257^3
+    nodes, the apply-roofline configuration), L2 scrubbed before each launch,
+    on the same lognormal field family; not part of the headline metric."""
+    from mnhack8_b200 import _lib
+    N = GATE_N
+    nodes, elems = (N + 1) ** 3, N ** 3
+    k, r = make_field(N, 1)
+    g = _lib.Solver(N, DT, k, r, kernel=kernel, scatter=scatter, detect=detect, no_source=True, ic="gaussian",
+                    ic_sigma=IC_SIGMA, rtol=RTOL, max_iter=500, device=device)
+    g.time_kernel(0, reps=3)
+    ms = min(g.time_kernel(0, reps=20) for _ in range(2))
+    g.close()
+    alg = (40 if detect else 32) * nodes + 16 * elems
+    peak, kind = peaks()
+    ach = alg / (ms * 1e-3) / 1e9
+    return {"N": N, "ms_per_launch": ms, "alg_bytes_per_launch": alg, "achieved": ach, "peak": peak,
+            "unit": "GB/s", "frac": ach / peak, "peak_source": f"{kind} hbm_gbs", "l2": "flushed before each launch"}
 
 
 def _initial(g, N):
