@@ -249,7 +249,7 @@ typedef struct hs_batch_options {
     int tile_planes;      /* operator tiles span min(N+1, tile_planes) planes; 0: a depth set by N
                              alone (the instance by itself fills the GPU, within 8..32 planes) */
     int device;
-    int pad;
+    int extrapolate;      /* start each step (after the first) from 2 T - T_prev instead of T */
 } hs_batch_options;
 typedef struct hs_batch_inst_info {
     int N, steps_done, steps_left, pad;

@@ -69,7 +69,7 @@ class FlipRecord(C.Structure):
 
 class BatchOptions(C.Structure):
     _fields_ = [("rtol", C.c_double), ("inner_tol", C.c_double), ("max_outer", C.c_int), ("max_inner", C.c_int),
-                ("detect", C.c_int), ("tile_planes", C.c_int), ("device", C.c_int), ("pad", C.c_int)]
+                ("detect", C.c_int), ("tile_planes", C.c_int), ("device", C.c_int), ("extrapolate", C.c_int)]
 
 
 class BatchFault(C.Structure):
@@ -398,11 +398,12 @@ class Batch:
     advance one implicit-Euler step per step() call, all in one graph launch."""
 
     def __init__(self, rtol=1e-8, inner_tol=1e-4, max_outer=10, max_inner=500, detect=True, tile_planes=0,
-                 device=0):
+                 device=0, extrapolate=True):
         o = BatchOptions()
         lib().hs_batch_default_options(C.byref(o))
         o.rtol, o.inner_tol, o.max_outer, o.max_inner = rtol, inner_tol, max_outer, max_inner
         o.detect, o.tile_planes, o.device = int(detect), int(tile_planes), int(device)
+        o.extrapolate = int(extrapolate)
         self._h = C.c_void_p()
         check(lib().hs_batch_create(C.byref(o), C.byref(self._h)))
         self.Nn = {}

@@ -5,6 +5,7 @@
 // one handle and advance together: hs_batch_step runs one implicit-Euler step
 // of every instance that has steps left, as one CUDA-graph launch:
 //   b = M T (FP64 slab operator, ABFT checked);
+//   start from T, or from 2 T - T_prev (extrapolate, from the second step);
 //   r = b - A T (FP64 slab operator, ABFT checked), test ||r|| / ||b|| < rtol;
 //   while not converged (bounded by max_outer):
 //       FP32 Jacobi-PCG on A d = r to inner_tol (bounded by max_inner),
@@ -116,6 +117,7 @@ BatchArgs batch_args(hs_batch* b) {
     a.rtol = b->opt.rtol; a.inner_tol = b->opt.inner_tol;
     a.max_outer = b->opt.max_outer; a.max_inner = b->opt.max_inner;
     a.detect = b->opt.detect;
+    a.extrapolate = b->opt.extrapolate;
     return a;
 }
 
@@ -180,6 +182,7 @@ hs_status build_batch_graph(hs_batch* b) {
     kb_step_begin<<<(a.n_inst + 127) / 128, 128, 0, b->s>>>(a);
     kb_apply<double, BK_RHS><<<(int)a.ntiles, ST, sizeof(BSlabSmem<double>), b->s>>>(a);
     kb_final_apply<BK_RHS><<<a.n_inst, RT, 0, b->s>>>(a);
+    kb_extrapolate<<<(int)a.nflat, RT, 0, b->s>>>(a);
     enqueue_resid(b, a);
     kb_cond<0><<<1, 1024, 0, b->s>>>(a, c_out, nullptr);
     HS_CUDA(cudaStreamEndCapture(b->s, &pre));
@@ -249,6 +252,7 @@ hs_status step_direct(hs_batch* b) {
     kb_step_begin<<<(a.n_inst + 127) / 128, 128, 0, b->s>>>(a);
     kb_apply<double, BK_RHS><<<(int)a.ntiles, ST, sizeof(BSlabSmem<double>), b->s>>>(a);
     kb_final_apply<BK_RHS><<<a.n_inst, RT, 0, b->s>>>(a);
+    kb_extrapolate<<<(int)a.nflat, RT, 0, b->s>>>(a);
     enqueue_resid(b, a);
     kb_cond<0><<<1, 1024, 0, b->s>>>(a, 0, flag.p);
     for (;;) {
@@ -281,7 +285,7 @@ void hs_batch_default_options(hs_batch_options* o) {
     if (!o) return;
     std::memset(o, 0, sizeof(*o));
     o->rtol = 1e-8; o->inner_tol = 1e-4; o->max_outer = 10; o->max_inner = 500;
-    o->detect = 1; o->tile_planes = 0; o->device = 0;
+    o->detect = 1; o->tile_planes = 0; o->device = 0; o->extrapolate = 1;
 }
 
 hs_status hs_batch_create(const hs_batch_options* opt, hs_batch** out) {
@@ -344,13 +348,14 @@ hs_status hs_batch_add(hs_batch* b, int N, double dt, const double* k, const dou
     // one allocation: FP64 node vectors T b y r wA wM diag, coefficients, FP32 vectors
     const size_t v8 = align256(Nn * 8), v4 = align256(Nn * 4), e16 = align256(Ne * 16), e8 = align256(Ne * 8),
                  e8b = align256(Ne * 8);
-    const size_t bytes = 7 * v8 + e16 + e8 + 2 * e8b + 7 * v4;
+    const size_t bytes = 8 * v8 + e16 + e8 + 2 * e8b + 7 * v4;
     void* mem = nullptr;
     HS_CUDA(cudaMalloc(&mem, bytes));
     char* q = (char*)mem;
     auto take = [&](size_t n) { char* r = q; q += n; return r; };
     BInst d{};
     d.T = (double*)take(v8); d.b = (double*)take(v8); d.y64 = (double*)take(v8); d.r64 = (double*)take(v8);
+    d.Tm1 = (double*)take(v8);
     double* wA = (double*)take(v8); double* wM = (double*)take(v8); double* diag = (double*)take(v8);
     d.coef64 = (const double2*)take(e16); d.coef32 = (const float2*)take(e8);
     double* rh = (double*)take(e8b); double* kk = (double*)take(e8b);

@@ -32,6 +32,8 @@ struct BState {
     int stalls;             // steps that ended at max_outer without reaching rtol
     int inner_bad;          // the current inner solve went non-finite: its correction is discarded
     int inner_faults;       // inner solves discarded so far
+    int has_prev;           // the previous step's field is kept (extrapolated start)
+    int extrap;             // this step starts from 2 T - T_prev
 };
 
 __device__ __forceinline__ float flipf(float x, int bit) {
@@ -54,6 +56,7 @@ struct BInst {
     double* b;                 // right-hand side M T_old
     double* y64;               // FP64 operator output
     double* r64;               // FP64 residual
+    double* Tm1;               // field at the start of the previous step (extrapolated start)
     const double2* coef64;     // (rho*c, k) per element
     const float2* coef32;
     const double* wA;          // ABFT weights A 1_int, M 1_int (FP64)
@@ -78,7 +81,7 @@ struct BatchArgs {
     double* pf;                // flat partials:  [q * nflat + block]
     double rtol, inner_tol;
     int max_outer, max_inner;
-    int detect, pad2;
+    int detect, extrapolate;
 };
 
 template <typename V> struct VTraits;
@@ -564,6 +567,24 @@ __global__ void kb_step_begin(BatchArgs B) {
     if (!I.active) return;
     BState* st = I.st;
     st->outer = 0; st->odone = 0; st->done = 1; st->iter = 0;
+    st->extrap = B.extrapolate && st->has_prev;
+    st->has_prev = 1;
+}
+
+// start of the step's solve (after b = M T): T <- 2 T - T_prev where a
+// previous field exists, else T unchanged; T_prev <- T of this step's start
+__global__ void __launch_bounds__(RT) kb_extrapolate(BatchArgs B) {
+    const FlatPos f = flat_pos(B);
+    if (f.slot < 0 || !B.extrapolate) return;
+    const BInst& I = B.inst[f.slot];
+    if (!I.active) return;
+    const bool ex = I.st->extrap;
+    for (int k = 0; k < f.cnt; ++k) {
+        const long long m = f.m0 + k;
+        const double t = I.T[m];
+        if (ex) I.T[m] = dfma(2.0, t, -I.Tm1[m]);
+        I.Tm1[m] = t;
+    }
 }
 
 // loop conditions: any active instance still in its outer loop (WHICH 0) /

@@ -67,7 +67,7 @@ def lognormal_many(jobs, workers=None):
 def batch_bytes(N):
     """Device bytes of one batched instance (the allocation hs_batch_add makes)."""
     Nn, Ne = (N + 1) ** 3, N ** 3
-    return 7 * 8 * Nn + 7 * 4 * Nn + 48 * Ne + 16 * 256
+    return 8 * 8 * Nn + 7 * 4 * Nn + 48 * Ne + 17 * 256
 
 
 def fp64_solve(N, k, r, steps, rtol, device=0):

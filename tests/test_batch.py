@@ -197,3 +197,24 @@ def test_direct_launches_equal_graph():
                          text=True, timeout=300, cwd=root)
     assert out.returncode == 0, out.stderr[-2000:]
     assert out.stdout.strip().splitlines()[-1] == want
+
+
+def test_extrapolated_start_same_answer_fewer_iterations(oracle):
+    """Starting each step from 2 T - T_prev changes where the solve starts, not
+    what it converges to: the fields agree within the tolerance and the inner
+    iterations do not grow."""
+    N, dt, steps = 16, 5e-4, 8
+    k, r = field(N, "lognormal", sigma=1.0, L=0.25, seed=12)
+    T0 = gaussian_T0(oracle, N, dt, k, r)
+    out = {}
+    for ex in (False, True):
+        b = _lib.Batch(rtol=1e-9, extrapolate=ex)
+        s = b.add(N, dt, k, r, T0=T0, steps=steps)
+        while b.step()[0]:
+            pass
+        out[ex] = (b.field(s), b.info(s))
+        b.close()
+    (T0f, i0), (T1f, i1) = out[False], out[True]
+    assert np.linalg.norm(T1f - T0f) <= 1e-8 * np.linalg.norm(T0f)
+    assert i1["rel_residual"] < 1e-9 and i0["rel_residual"] < 1e-9
+    assert i1["inner_iters"] <= i0["inner_iters"]
