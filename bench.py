@@ -64,6 +64,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-gate", action="store_true",
                     help="skip the supplementary N=256 operator-kernel measurement")
+    ap.add_argument("--serving-requests", type=int, default=48,
+                    help="requests of the supplementary serving measurement (0: skip)")
     ap.add_argument("--profile", action="store_true",
                     help="only the timed trajectories (no e2e, kernel timing or CPU baseline): for ncu captures")
     return ap.parse_args()
@@ -345,6 +347,8 @@ def main():
     }
     if rank == 0 and not args.no_gate and N != GATE_N:
         line["apply_gate_N256"] = gate_apply(local, detect, args.kernel, args.scatter)
+    if rank == 0 and world == 1 and args.serving_requests > 0:
+        line["serving"] = serving_leg(args.serving_requests, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sample(N, args.cpu_seconds)
     if rank == 0:
@@ -357,6 +361,17 @@ def main():
 
 
 GATE_N = 256
+
+
+def serving_leg(n, device):
+    """Supplementary: served solves/s and p50 / p99 latency of the batched
+    mixed-precision server beside serial plain FP64 on this GPU, for the first
+    n requests of the seeded serving stream (Poisson 200/s, N 16..160, 10..100
+    steps, 30 % flipped, rtol 1e-8); fields are generated before timing."""
+    from mnhack8_b200 import ensemble
+    r = ensemble.serving(n=n, device=device)
+    return {"requests": n, "stream": "Poisson 200/s, N 16..160, steps 10..100, 30% one bit flip, rtol 1e-8",
+            "batched": r["batched"], "serial_fp64": r["serial_fp64"], "solves_per_s_ratio": r["throughput_ratio"]}
 
 
 def gate_apply(device, detect, kernel, scatter):
