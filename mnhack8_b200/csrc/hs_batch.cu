@@ -21,13 +21,16 @@
 
 namespace {
 
-// tile shape of one batched instance: C, R as in the slab layout (largest
-// tile plane that fits, fewest positions loaded per node) and CX planes per
-// tile: min(N+1, planes), or with planes == 0 a function of N alone (the
-// depth at which the instance by itself fills SLAB_SLOTS tiles, within 8..32),
-// so that an instance's arithmetic never depends on the rest of the batch
+// tile shape of one batched instance, a function of N and planes alone so that
+// an instance's arithmetic never depends on the rest of the batch.  planes == 0:
+// an instance large enough to fill the GPU by itself with tiles of at least 8
+// planes takes the single-instance slab layout (the FP64 operator's, whose
+// cost model counts waves over SLAB_SLOTS); a smaller one takes C, R with the
+// fewest positions loaded per node and the depth at which it would fill
+// SLAB_SLOTS tiles, within 8..32.  planes > 0: those C, R and min(N+1, planes).
 Part batch_part(int N, int planes) {
     const long long NN = N + 1;
+    if (planes < 1 && slab_layout(N).CX >= 8) return make_part(N);
     long long bestC = NN, bestR = 1, best_cost = -1;
     const long long cmin = NN < 30 ? NN : 30;
     for (long long C = cmin; C <= NN; ++C) {

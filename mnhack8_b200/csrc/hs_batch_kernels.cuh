@@ -328,7 +328,7 @@ __global__ void __launch_bounds__(ST, 2) kb_apply(BatchArgs B) {
 template <int NQ>
 __device__ __forceinline__ void inst_sums(double (&v)[NQ], const double* base, long long count, long long qstride,
                                           double (*sh)[8]) {
-    constexpr int FB = 8;
+    constexpr int FB = 16;
 #pragma unroll
     for (int q = 0; q < NQ; ++q) v[q] = 0.0;
     for (long long k0 = threadIdx.x; k0 < count; k0 += (long long)RT * FB) {
@@ -482,15 +482,43 @@ __global__ void __launch_bounds__(RT) kb_update32(BatchArgs B) {
             const float alpha = (float)st->alpha;
             const float* p = (iter & 1) ? I.p32b : I.p32a;
             const bool fr = fi_now(st, FI_RV);
-            for (int k = 0; k < f.cnt; ++k) {
-                const long long m = f.m0 + k;
-                I.d32[m] = __fmaf_rn(alpha, p[m], I.d32[m]);
-                float r = __fmaf_rn(-alpha, I.Ap32[m], I.r32[m]);
-                if (fr && m == st->fi_idx) { r = flipf(r, st->fi_bit); I.st->fi_fired = 1; }
-                const float z = __fmul_rn(r, I.dinv32[m]);
-                I.r32[m] = r; I.z32[m] = z;
-                part[0] = dfma((double)r, (double)r, part[0]);
-                part[1] = dfma((double)r, (double)z, part[1]);
+            // the thread's node pair as 8-byte vectors (m0 is even, the buffers 256-byte aligned)
+            float dv[2], pv[2], qv[2], rv[2], iv[2];
+            if (f.cnt == 2) {
+                const float2 a = *reinterpret_cast<const float2*>(I.d32 + f.m0);
+                const float2 b = *reinterpret_cast<const float2*>(p + f.m0);
+                const float2 c = *reinterpret_cast<const float2*>(I.Ap32 + f.m0);
+                const float2 d = *reinterpret_cast<const float2*>(I.r32 + f.m0);
+                const float2 e = __ldg(reinterpret_cast<const float2*>(I.dinv32 + f.m0));
+                dv[0] = a.x; dv[1] = a.y; pv[0] = b.x; pv[1] = b.y; qv[0] = c.x; qv[1] = c.y;
+                rv[0] = d.x; rv[1] = d.y; iv[0] = e.x; iv[1] = e.y;
+            } else {
+                for (int k = 0; k < 2; ++k) {
+                    const bool in = k < f.cnt;
+                    const long long m = f.m0 + k;
+                    dv[k] = in ? I.d32[m] : 0.f; pv[k] = in ? p[m] : 0.f; qv[k] = in ? I.Ap32[m] : 0.f;
+                    rv[k] = in ? I.r32[m] : 0.f; iv[k] = in ? I.dinv32[m] : 0.f;
+                }
+            }
+            float zv[2];
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                dv[k] = __fmaf_rn(alpha, pv[k], dv[k]);
+                float r = __fmaf_rn(-alpha, qv[k], rv[k]);
+                if (fr && f.m0 + k == st->fi_idx && k < f.cnt) { r = flipf(r, st->fi_bit); I.st->fi_fired = 1; }
+                rv[k] = r;
+                zv[k] = __fmul_rn(r, iv[k]);
+                if (k < f.cnt) {
+                    part[0] = dfma((double)r, (double)r, part[0]);
+                    part[1] = dfma((double)r, (double)zv[k], part[1]);
+                }
+            }
+            if (f.cnt == 2) {
+                *reinterpret_cast<float2*>(I.d32 + f.m0) = make_float2(dv[0], dv[1]);
+                *reinterpret_cast<float2*>(I.r32 + f.m0) = make_float2(rv[0], rv[1]);
+                *reinterpret_cast<float2*>(I.z32 + f.m0) = make_float2(zv[0], zv[1]);
+            } else if (f.cnt == 1) {
+                I.d32[f.m0] = dv[0]; I.r32[f.m0] = rv[0]; I.z32[f.m0] = zv[0];
             }
         }
     }

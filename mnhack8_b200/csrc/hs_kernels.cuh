@@ -262,7 +262,7 @@ __device__ __forceinline__ void store_partials(double (&v)[NQ], double* partials
 // few memory latencies instead of one per partial.
 template <int NQ>
 __device__ __forceinline__ void final_sums(double (&v)[NQ], const double* partials, long long nblk, double (*sh)[8]) {
-    constexpr int FB = 8;
+    constexpr int FB = 16;
 #pragma unroll
     for (int q = 0; q < NQ; ++q) v[q] = 0.0;
     for (long long k0 = threadIdx.x; k0 < nblk; k0 += (long long)RT * FB) {
