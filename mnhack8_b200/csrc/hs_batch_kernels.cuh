@@ -136,18 +136,11 @@ struct __align__(16) BSlabSmem {
 // Partials per tile: p.Ap (KIND 2), and D1: 1_int.y, w.x, x.x.
 enum BKind { BK_RESID = 0, BK_RHS = 1, BK_LOOP = 2 };
 
-template <typename V, int KIND>
-__global__ void __launch_bounds__(ST, 2) kb_apply(BatchArgs B) {
+// tile t of instance I; FI false: no vector fault is armed for this launch
+template <typename V, int KIND, bool FI>
+__device__ __forceinline__ void kb_tile(const BatchArgs& B, BSlabSmem<V>& S, long long t, const BInst& I) {
     using T2 = typename VTraits<V>::V2;
     using VT = VTraits<V>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    BSlabSmem<V>& S = *reinterpret_cast<BSlabSmem<V>*>(smem_raw);
-    const long long t = blockIdx.x;
-    if (t >= B.ntiles) return;
-    const int slot = B.tile2inst[t];
-    if (slot < 0) return;
-    const BInst& I = B.inst[slot];
-    if (!I.active) return;
     BState* st = I.st;
     const bool loop = KIND == BK_LOOP;
     if constexpr (KIND == BK_LOOP) {
@@ -157,7 +150,8 @@ __global__ void __launch_bounds__(ST, 2) kb_apply(BatchArgs B) {
     }
     const Part& P = I.part;
     const int N = P.N, Cw = P.Cw;
-    const long long plane = (long long)P.NN * P.NN, eplane = (long long)N * N;
+    // node and element indices fit in 32 bits (N <= 1200)
+    const unsigned plane = (unsigned)P.NN * (unsigned)P.NN, eplane = (unsigned)N * (unsigned)N;
     const SlabTile Tt = slab_tile(P, t - I.tile0);
     const SlabPos G = slab_pos(P, Tt, threadIdx.x);
     const unsigned fl = G.fl;
@@ -195,24 +189,25 @@ __global__ void __launch_bounds__(ST, 2) kb_apply(BatchArgs B) {
     double wv[SK];
     auto ld_raw = [&](int px) {
         const bool pv = px >= 0 && px <= N;
-        const long long base = (long long)px * plane;
+        const unsigned base = (unsigned)px * plane;
 #pragma unroll
         for (int k = 0; k < SK; ++k) {
             const bool v = pv && sp_valid(fl, k);
-            ra[k] = v ? src_a[base + G.noff[k]] : (V)0;
-            rb[k] = (v && two) ? src_b[base + G.noff[k]] : (V)0;
+            const unsigned n = base + (unsigned)G.noff[k];
+            ra[k] = v ? __ldg(src_a + n) : (V)0;
+            rb[k] = (v && two) ? __ldg(src_b + n) : (V)0;
         }
     };
     int fi_p = 0, fi_ap = 0, fi_bit = 0;
     long long fi_idx = -1;
-    if constexpr (KIND == BK_LOOP) {
+    if constexpr (KIND == BK_LOOP && FI) {
         fi_p = fi_now(st, FI_P); fi_ap = fi_now(st, FI_AP);
         fi_bit = st->fi_bit; fi_idx = st->fi_idx;
     }
     auto form = [&](V (&p)[SK], int px) {
 #pragma unroll
         for (int k = 0; k < SK; ++k) p[k] = two ? VT::fma(beta, rb[k], ra[k]) : ra[k];
-        if constexpr (KIND == BK_LOOP) {
+        if constexpr (KIND == BK_LOOP && FI) {
             if (fi_p) {
 #pragma unroll
                 for (int k = 0; k < SK; ++k)
@@ -225,24 +220,26 @@ __global__ void __launch_bounds__(ST, 2) kb_apply(BatchArgs B) {
     };
     auto ld_coef = [&](int ex) {
         const bool ev = ex >= 0 && ex < N;
-        const long long base = (long long)ex * eplane;
+        const unsigned base = (unsigned)ex * eplane;
 #pragma unroll
         for (int k = 0; k < SK; ++k) {
             const bool v = ev && sp_elem(fl, k);
+            const unsigned e = base + (unsigned)G.eoff[k];
             if constexpr (sizeof(V) == 4) {
-                const float2 c = v ? __ldg(I.coef32 + base + G.eoff[k]) : make_float2(0.f, 0.f);
+                const float2 c = v ? __ldg(I.coef32 + e) : make_float2(0.f, 0.f);
                 cr[k] = c.x; ckk[k] = c.y;
             } else {
-                const double2 c = v ? __ldg(I.coef64 + base + G.eoff[k]) : make_double2(0.0, 0.0);
+                const double2 c = v ? __ldg(I.coef64 + e) : make_double2(0.0, 0.0);
                 cr[k] = c.x; ckk[k] = c.y;
             }
         }
     };
     auto ld_w = [&](int px) {
         const bool pv = px >= xa && px <= xb;
-        const long long base = (long long)px * plane;
+        const unsigned base = (unsigned)px * plane;
 #pragma unroll
-        for (int k = 0; k < SK; ++k) wv[k] = (pv && d1 && sp_out(fl, k)) ? __ldg(w + base + G.noff[k]) : 0.0;
+        for (int k = 0; k < SK; ++k)
+            wv[k] = (pv && d1 && sp_out(fl, k)) ? __ldg(w + (base + (unsigned)G.noff[k])) : 0.0;
     };
     auto layer = [&](int ix, int cur, V (&pc)[SK], V (&pn)[SK], V (&ac)[SK], V (&an)[SK]) {
         const int nxt = cur ^ 1;
@@ -275,7 +272,7 @@ __global__ void __launch_bounds__(ST, 2) kb_apply(BatchArgs B) {
         }
         ld_coef(ix + 1 <= xb ? ix + 1 : -1);
         __syncthreads();
-        const long long base = (long long)ix * plane;
+        const unsigned base = (unsigned)ix * plane;
         const bool xbnd = ix == 0 || ix == N;
 #pragma unroll
         for (int k = 0; k < SK; ++k) {
@@ -285,11 +282,11 @@ __global__ void __launch_bounds__(ST, 2) kb_apply(BatchArgs B) {
             T2 y3{(V)0, (V)0}, y2 = y3, y1 = y3;
             if (yzin) { y3 = S.Y3[j]; y2 = S.Y2[j]; y1 = S.Y1[j]; }
             if (ix >= xa) {
-                const long long n = base + G.noff[k];
+                const unsigned n = base + (unsigned)G.noff[k];
                 const bool bnd = !yzin || xbnd;
                 V y = bnd ? (V)0 : VT::add(VT::add(VT::add(ac[k], y3.x), y2.x), y1.x);
-                if constexpr (KIND == BK_LOOP) {
-                    if (fi_ap && n == fi_idx) { y = flipf(y, fi_bit); st->fi_fired = 1; }
+                if constexpr (KIND == BK_LOOP && FI) {
+                    if (fi_ap && (long long)n == fi_idx) { y = flipf(y, fi_bit); st->fi_fired = 1; }
                 }
                 const double pv = (double)pc[k], yd = (double)y;
                 if (loop) part[0] = dfma(pv, yd, part[0]);
@@ -298,8 +295,8 @@ __global__ void __launch_bounds__(ST, 2) kb_apply(BatchArgs B) {
                     part[2] = dfma(wv[k], pv, part[2]);
                     part[3] = dfma(pv, pv, part[3]);
                 }
-                yout[n] = y;
-                if (loop) pout[n] = pc[k];
+                __stwb(yout + n, y);                      // global stores (the pointers come from global memory)
+                if (loop) __stwb(pout + n, pc[k]);
             }
             an[k] = yzin ? VT::add(VT::add(VT::add(an[k], y3.y), y2.y), y1.y) : (V)0;
         }
@@ -321,6 +318,24 @@ __global__ void __launch_bounds__(ST, 2) kb_apply(BatchArgs B) {
     if (threadIdx.x == 0) {
 #pragma unroll
         for (int q = 0; q < MAXQ; ++q) B.pa[q * B.ntiles + t] = part[q];
+    }
+}
+
+template <typename V, int KIND>
+__global__ void __launch_bounds__(ST, 2) kb_apply(BatchArgs B) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    BSlabSmem<V>& S = *reinterpret_cast<BSlabSmem<V>*>(smem_raw);
+    const long long t = blockIdx.x;
+    if (t >= B.ntiles) return;
+    const int slot = B.tile2inst[t];
+    if (slot < 0) return;
+    const BInst& I = B.inst[slot];
+    if (!I.active) return;
+    if constexpr (KIND == BK_LOOP) {
+        if (fi_now(I.st, FI_P) || fi_now(I.st, FI_AP)) kb_tile<V, KIND, true>(B, S, t, I);
+        else kb_tile<V, KIND, false>(B, S, t, I);
+    } else {
+        kb_tile<V, KIND, false>(B, S, t, I);
     }
 }
 

@@ -330,16 +330,19 @@ struct __align__(16) SlabSmem {
 };
 constexpr size_t kSlabSmem = sizeof(SlabSmem);
 
-// MODE 0: input x as given; 1: PCG loop, p = z; 2: PCG loop, p = z + beta p_{k-1}
-template <int FORM, int MODE>
+// MODE 0: input x as given; 1: PCG loop, p = z; 2: PCG loop, p = z + beta p_{k-1}.
+// FI false: no fault is armed for this launch (the per-node fault tests compile out).
+template <int FORM, int MODE, bool FI = true>
 __device__ __forceinline__ void slab_march(const ApplyArgs& a, SlabSmem& S, const SlabTile& T, const SlabPos& G,
                                            const double* src_a, const double* src_b, double beta, double* pout,
                                            bool loop, bool d1, bool rhs, int fi_p, int fi_ap, int fi_r, int fi_bit,
                                            long long fi_idx, long long fi_elem, double (&part)[MAXQ]) {
     constexpr bool TWO = MODE == 2;
+    if (!FI) { fi_p = 0; fi_ap = 0; fi_r = 0; }
     const Part& P = a.part;
     const int N = P.N, Cw = P.Cw;
-    const long long plane = (long long)P.NN * P.NN, eplane = (long long)N * N;
+    // node and element indices fit in 32 bits (N <= 1200): one wide multiply-add per address
+    const unsigned plane = (unsigned)P.NN * (unsigned)P.NN, eplane = (unsigned)N * (unsigned)N;
     const int tid = threadIdx.x;
     const unsigned fl = G.fl;
     const int xa = T.xa, xb = T.xb;
@@ -347,42 +350,42 @@ __device__ __forceinline__ void slab_march(const ApplyArgs& a, SlabSmem& S, cons
     double pA[SK], pB[SK], aA[SK], aB[SK], ra[SK], rb[SK], cr[SK], ck[SK], wv[SK], fv[SK];
     auto ld_raw = [&](int px) {
         const bool pv = px >= 0 && px <= N;
-        const double* sa = src_a + (long long)px * plane;
-        const double* sb = TWO ? src_b + (long long)px * plane : nullptr;
+        const unsigned base = (unsigned)px * plane;
 #pragma unroll
         for (int k = 0; k < SK; ++k) {
             const bool v = pv && sp_valid(fl, k);
-            ra[k] = v ? __ldg(sa + G.noff[k]) : 0.0;
-            if (TWO) rb[k] = v ? __ldg(sb + G.noff[k]) : 0.0;
+            const unsigned n = base + (unsigned)G.noff[k];
+            ra[k] = v ? __ldg(src_a + n) : 0.0;
+            if (TWO) rb[k] = v ? __ldg(src_b + n) : 0.0;
         }
     };
     auto form = [&](int px, double (&p)[SK]) {
-        const long long base = (long long)px * plane;
 #pragma unroll
         for (int k = 0; k < SK; ++k) {
             double v = TWO ? dfma(beta, rb[k], ra[k]) : ra[k];
-            if (fi_p && sp_valid(fl, k) && base + G.noff[k] == fi_idx) v = flipbit(v, fi_bit);
+            if (fi_p && sp_valid(fl, k) && (long long)px * plane + G.noff[k] == fi_idx) v = flipbit(v, fi_bit);
             p[k] = v;
         }
     };
     auto ld_coef = [&](int ex) {
         const bool ev = ex >= 0 && ex < N;
-        const double2* ce = a.coef + (long long)ex * eplane;
+        const unsigned base = (unsigned)ex * eplane;
 #pragma unroll
         for (int k = 0; k < SK; ++k) {
             const bool v = ev && sp_elem(fl, k);
-            const double2 c = v ? __ldg(ce + G.eoff[k]) : make_double2(0.0, 0.0);
+            const double2 c = v ? __ldg(a.coef + (base + (unsigned)G.eoff[k])) : make_double2(0.0, 0.0);
             cr[k] = c.x; ck[k] = c.y;
         }
     };
     auto ld_w = [&](int px) {
         const bool pv = px >= xa && px <= xb;
-        const long long base = (long long)px * plane;
+        const unsigned base = (unsigned)px * plane;
 #pragma unroll
         for (int k = 0; k < SK; ++k) {
             const bool v = pv && sp_out(fl, k);
-            wv[k] = (v && d1) ? __ldg(a.w + base + G.noff[k]) : 0.0;
-            if (MODE == 0) fv[k] = (v && rhs) ? __ldg(a.F + base + G.noff[k]) : 0.0;
+            const unsigned n = base + (unsigned)G.noff[k];
+            wv[k] = (v && d1) ? __ldg(a.w + n) : 0.0;
+            if (MODE == 0) fv[k] = (v && rhs) ? __ldg(a.F + n) : 0.0;
         }
     };
 
@@ -424,7 +427,7 @@ __device__ __forceinline__ void slab_march(const ApplyArgs& a, SlabSmem& S, cons
         ld_coef(ix + 1 <= xb ? ix + 1 : -1);
         __syncthreads();
         // 3. tile nodes of plane ix; node sums of plane ix+1
-        const long long base = (long long)ix * plane;
+        const unsigned base = (unsigned)ix * plane;
         const bool xbnd = ix == 0 || ix == N;
 #pragma unroll
         for (int k = 0; k < SK; ++k) {
@@ -434,10 +437,10 @@ __device__ __forceinline__ void slab_march(const ApplyArgs& a, SlabSmem& S, cons
             double2 y3 = make_double2(0.0, 0.0), y2 = y3, y1 = y3;
             if (yzin) { y3 = S.Y3[j]; y2 = S.Y2[j]; y1 = S.Y1[j]; }
             if (ix >= xa) {
-                const long long n = base + G.noff[k];
+                const unsigned n = base + (unsigned)G.noff[k];
                 const bool bnd = !yzin || xbnd;
                 double y = bnd ? 0.0 : dadd(dadd(dadd(ac[k], y3.x), y2.x), y1.x);
-                if (fi_ap && n == fi_idx) y = flipbit(y, fi_bit);
+                if (fi_ap && (long long)n == fi_idx) y = flipbit(y, fi_bit);
                 const double pv = pc[k];
                 if (loop) part[0] = dfma(pv, y, part[0]);
                 if (d1) {
@@ -496,9 +499,11 @@ __global__ void __launch_bounds__(ST, FORM == FORM_WHT ? 2 : 1) k_apply_slab(App
         if (!src_b)
             slab_march<FORM, 1>(a, S, T, G, a.z, src_b, beta, pout, true, d1, false, fi_p, fi_ap, 0, fi_bit, fi_idx,
                                 -1, part);
+        else if (fi_p || fi_ap)
+            slab_march<FORM, 2, true>(a, S, T, G, a.z, src_b, beta, pout, true, d1, false, fi_p, fi_ap, 0, fi_bit,
+                                      fi_idx, -1, part);
         else
-            slab_march<FORM, 2>(a, S, T, G, a.z, src_b, beta, pout, true, d1, false, fi_p, fi_ap, 0, fi_bit, fi_idx,
-                                -1, part);
+            slab_march<FORM, 2, false>(a, S, T, G, a.z, src_b, beta, pout, true, d1, false, 0, 0, 0, 0, -1, -1, part);
     } else {
         if (a.role == ROLE_X0 && st->fi_armR) { fi_r = 1; fi_elem = st->fi_elem; fi_bit = st->fi_bit; }
         const bool rhs = (a.role == ROLE_RHS) && a.F != nullptr;
