@@ -279,6 +279,15 @@ hs_status hs_batch_arm_fault(hs_batch* b, int slot, const hs_batch_fault* f);
 hs_status hs_batch_remove(hs_batch* b, int slot);
 /* one step of every instance with steps left; device time of the launch */
 hs_status hs_batch_step(hs_batch* b, int* n_active, double* device_ms);
+/* hs_batch_step in two halves, so that the host can admit instances while the
+ * step runs: _begin launches the step of every instance with steps left and
+ * returns at once; _end waits for it (*n_stepped instances, device time).
+ * Between them hs_batch_add sets up new instances on a stream of its own (they
+ * join at the next step), and hs_batch_remove frees an instance after the step
+ * (its slot is reused only once the step has ended).  A second _begin before
+ * _end is an error. */
+hs_status hs_batch_step_begin(hs_batch* b, int* n_active);
+hs_status hs_batch_step_end(hs_batch* b, int* n_stepped, double* device_ms);
 hs_status hs_batch_info(hs_batch* b, int slot, hs_batch_inst_info* out);
 hs_status hs_batch_get_field(hs_batch* b, int slot, double* T_host);
 

@@ -26,7 +26,8 @@ EXPORTS = [
     "hs_arm_fi", "hs_run_case", "hs_verify", "hs_solve_host", "hs_diag_cg", "hs_set_dump", "hs_set_case_tag",
     "hs_target_on_boundary", "hs_classify", "hs_cli_main", "hs_advance", "hs_set_field", "hs_get_field",
     "hs_time_kernel", "hs_dot_noalloc", "hs_campaign", "hs_batch_default_options", "hs_batch_create",
-    "hs_batch_destroy", "hs_batch_add", "hs_batch_arm_flip", "hs_batch_arm_fault", "hs_batch_remove", "hs_batch_step", "hs_batch_info", "hs_batch_get_field", "hs_gaussian_ic",
+    "hs_batch_destroy", "hs_batch_add", "hs_batch_arm_flip", "hs_batch_arm_fault", "hs_batch_remove", "hs_batch_step",
+    "hs_batch_step_begin", "hs_batch_step_end", "hs_batch_info", "hs_batch_get_field", "hs_gaussian_ic",
 ]
 
 
@@ -172,6 +173,10 @@ def lib():
     L.hs_batch_remove.argtypes = [vp, i]
     L.hs_batch_step.restype = i
     L.hs_batch_step.argtypes = [vp, C.POINTER(i), pd]
+    L.hs_batch_step_begin.restype = i
+    L.hs_batch_step_begin.argtypes = [vp, C.POINTER(i)]
+    L.hs_batch_step_end.restype = i
+    L.hs_batch_step_end.argtypes = [vp, C.POINTER(i), pd]
     L.hs_batch_info.restype = i
     L.hs_batch_info.argtypes = [vp, i, C.POINTER(BatchInstInfo)]
     L.hs_batch_get_field.restype = i
@@ -435,6 +440,19 @@ class Batch:
         """One step of every instance with steps left: (instances stepped, device ms)."""
         n, ms = C.c_int(0), C.c_double(0.0)
         check(lib().hs_batch_step(self._h, C.byref(n), C.byref(ms)))
+        return n.value, ms.value
+
+    def step_begin(self):
+        """Launch one step of every instance with steps left and return at once
+        (instances in the step); add() and remove() may run until step_end()."""
+        n = C.c_int(0)
+        check(lib().hs_batch_step_begin(self._h, C.byref(n)))
+        return n.value
+
+    def step_end(self):
+        """Wait for the step in flight: (instances stepped, device ms)."""
+        n, ms = C.c_int(0), C.c_double(0.0)
+        check(lib().hs_batch_step_end(self._h, C.byref(n), C.byref(ms)))
         return n.value, ms.value
 
     def info(self, slot):

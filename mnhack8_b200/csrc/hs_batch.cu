@@ -78,12 +78,19 @@ struct hs_batch {
         Part part{};
         void* mem = nullptr;      // one allocation holding every buffer of the instance
         BInst desc{};
+        bool in_step = false;     // part of the step in flight
+        bool held = false;        // removed while a step was in flight: reusable after it ends
     };
     std::vector<Slot> slots;
     DevBuf<BInst> d_inst;
     DevBuf<BState> d_st;
     DevBuf<int> d_t2i, d_f2i;
     DevBuf<double> pa, pf;
+    DevBuf<double> sq, spart;     // set-up reductions of hs_batch_add
+    cudaMemPool_t pool = nullptr; // instance arenas: stream-ordered, kept reserved for reuse
+    cudaStream_t s_add = nullptr; // set-up of added instances, overlapping a step in flight
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    bool inflight = false;        // hs_batch_step_begin without its hs_batch_step_end
     long long cap_tiles = 0, cap_flat = 0;
     bool dirty = true;            // maps / descriptors need an upload
     cudaGraph_t graph = nullptr;
@@ -92,8 +99,12 @@ struct hs_batch {
     ~hs_batch() {
         if (gexec) cudaGraphExecDestroy(gexec);
         if (graph) cudaGraphDestroy(graph);
-        for (Slot& sl : slots) if (sl.mem) cudaFree(sl.mem);
-        if (s) cudaStreamDestroy(s);
+        for (Slot& sl : slots) if (sl.mem) cudaFreeAsync(sl.mem, s);
+        if (s) { cudaStreamSynchronize(s); cudaStreamDestroy(s); }
+        if (s_add) { cudaStreamSynchronize(s_add); cudaStreamDestroy(s_add); }
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (pool) cudaMemPoolDestroy(pool);
     }
 };
 
@@ -303,6 +314,18 @@ hs_status hs_batch_create(const hs_batch_options* opt, hs_batch** out) {
     auto b = std::make_unique<hs_batch>();
     b->opt = *opt;
     HS_CUDA(cudaStreamCreateWithFlags(&b->s, cudaStreamNonBlocking));
+    HS_CUDA(cudaStreamCreateWithFlags(&b->s_add, cudaStreamNonBlocking));
+    HS_CUDA(cudaEventCreate(&b->ev0));
+    HS_CUDA(cudaEventCreate(&b->ev1));
+    cudaMemPoolProps pp{};
+    pp.allocType = cudaMemAllocationTypePinned;
+    pp.location.type = cudaMemLocationTypeDevice;
+    pp.location.id = opt->device;
+    HS_CUDA(cudaMemPoolCreate(&b->pool, &pp));
+    uint64_t keep = UINT64_MAX;     // freed arenas stay with the pool for the next instances
+    HS_CUDA(cudaMemPoolSetAttribute(b->pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    int no = 0;                     // an add never waits on the step stream for a freed arena
+    HS_CUDA(cudaMemPoolSetAttribute(b->pool, cudaMemPoolReuseAllowInternalDependencies, &no));
     set_bsmem();
     *out = b.release();
     return HS_OK;
@@ -327,9 +350,15 @@ hs_status hs_batch_add(hs_batch* b, int N, double dt, const double* k, const dou
     const RefMatrices mats = build_reference_matrices(N);
     if (!mats.ok) { set_error("reference-matrix self-check failed"); return HS_ERR_MATRIX; }
     // slot
+    // A free slot is inactive in the descriptors of any step in flight (a slot
+    // removed during that step is held until it ends), so its state may be
+    // written on s_add while the step runs.  Growing the slot arrays replaces
+    // what the step reads: it waits for the step first.
     int slot = -1;
-    for (size_t i = 0; i < b->slots.size(); ++i) if (!b->slots[i].used) { slot = (int)i; break; }
+    for (size_t i = 0; i < b->slots.size(); ++i)
+        if (!b->slots[i].used && !b->slots[i].held) { slot = (int)i; break; }
     if (slot < 0) {
+        HS_CUDA(cudaStreamSynchronize(b->s));
         slot = (int)b->slots.size();
         b->slots.emplace_back();
         // descriptor and state arrays follow the slot count (the graph reads n_inst)
@@ -353,7 +382,8 @@ hs_status hs_batch_add(hs_batch* b, int N, double dt, const double* k, const dou
                  e8b = align256(Ne * 8);
     const size_t bytes = 8 * v8 + e16 + e8 + 2 * e8b + 7 * v4;
     void* mem = nullptr;
-    HS_CUDA(cudaMalloc(&mem, bytes));
+    cudaStream_t sa = b->s_add;
+    HS_CUDA(cudaMallocFromPoolAsync(&mem, bytes, b->pool, sa));
     char* q = (char*)mem;
     auto take = [&](size_t n) { char* r = q; q += n; return r; };
     BInst d{};
@@ -369,60 +399,43 @@ hs_status hs_batch_add(hs_batch* b, int N, double dt, const double* k, const dou
     d.dt = dt;
     for (int j = 0; j < 4; ++j) { d.cm[j] = mats.cm[j]; d.ck[j] = mats.ck[j]; d.cmf[j] = (float)mats.cm[j]; d.ckf[j] = (float)mats.ck[j]; }
     d.st = b->d_st.p + slot;
-    // coefficients, initial field
-    {
-        std::vector<double2> c64(Ne);
-        std::vector<float2> c32(Ne);
-        for (long long e = 0; e < Ne; ++e) {
-            c64[e] = make_double2(rhoc[e], k[e]);
-            c32[e] = make_float2((float)rhoc[e], (float)k[e]);
-        }
-        HS_CUDA(cudaMemcpyAsync((void*)d.coef64, c64.data(), Ne * 16, cudaMemcpyHostToDevice, b->s));
-        HS_CUDA(cudaMemcpyAsync((void*)d.coef32, c32.data(), Ne * 8, cudaMemcpyHostToDevice, b->s));
-        HS_CUDA(cudaMemcpyAsync(rh, rhoc, Ne * 8, cudaMemcpyHostToDevice, b->s));
-        HS_CUDA(cudaMemcpyAsync(kk, k, Ne * 8, cudaMemcpyHostToDevice, b->s));
-        if (T0) HS_CUDA(cudaMemcpyAsync(d.T, T0, Nn * 8, cudaMemcpyHostToDevice, b->s));
-        else HS_CUDA(cudaMemsetAsync(d.T, 0, Nn * 8, b->s));
-        HS_CUDA(cudaStreamSynchronize(b->s));
-    }
+    // coefficients (interleaved on the device), initial field
+    const int gn = (int)std::min<long long>((Nn + RT - 1) / RT, 1 << 30);
+    HS_CUDA(cudaMemcpyAsync(rh, rhoc, Ne * 8, cudaMemcpyHostToDevice, sa));
+    HS_CUDA(cudaMemcpyAsync(kk, k, Ne * 8, cudaMemcpyHostToDevice, sa));
+    if (T0) HS_CUDA(cudaMemcpyAsync(d.T, T0, Nn * 8, cudaMemcpyHostToDevice, sa));
+    else HS_CUDA(cudaMemsetAsync(d.T, 0, Nn * 8, sa));
+    k_pack_coef<<<grid_for(Ne, RT), RT, 0, sa>>>(Ne, rh, kk, (double2*)d.coef64, (float2*)d.coef32);
     // diagonal, ABFT weights and their norms (node-parallel operator, FP64)
     ElemConsts ec{};
     std::memcpy(ec.M, mats.M, sizeof(ec.M)); std::memcpy(ec.K, mats.K, sizeof(ec.K));
     std::memcpy(ec.cm, mats.cm, sizeof(ec.cm)); std::memcpy(ec.ck, mats.ck, sizeof(ec.ck));
     ec.detJ = mats.detJ;
-    const int gn = (int)std::min<long long>((Nn + RT - 1) / RT, 1 << 30);
     GenArgs ga{};
     ga.N = N; ga.kind = GEN_DIAG; ga.project = 1; ga.dt_eff = dt; ga.y = diag; ga.rhoc = rh; ga.kc = kk;
     ga.ec = ec; ga.fi_elem = -1;
-    k_apply_nodes<FORM_WHT><<<gn, RT, 0, b->s>>>(ga);
-    k_recip32<<<gn, RT, 0, b->s>>>(Nn, diag, (float*)d.dinv32);
-    k_ones_interior<<<gn, RT, 0, b->s>>>(N, d.r64);
+    k_apply_nodes<FORM_WHT><<<gn, RT, 0, sa>>>(ga);
+    k_recip32<<<gn, RT, 0, sa>>>(Nn, diag, (float*)d.dinv32);
+    k_ones_interior<<<gn, RT, 0, sa>>>(N, d.r64);
     GenArgs gw = ga;
     gw.kind = GEN_APPLY; gw.project = 0; gw.x = d.r64;
     gw.dt_eff = 0.0; gw.y = wM;
-    k_apply_nodes<FORM_WHT><<<gn, RT, 0, b->s>>>(gw);
+    k_apply_nodes<FORM_WHT><<<gn, RT, 0, sa>>>(gw);
     gw.dt_eff = dt; gw.y = wA;
-    k_apply_nodes<FORM_WHT><<<gn, RT, 0, b->s>>>(gw);
-    DevBuf<double> red;
-    HS_CUDA(red.alloc(4));
+    k_apply_nodes<FORM_WHT><<<gn, RT, 0, sa>>>(gw);
     const long long nflat = (Nn + (long long)RT * KF - 1) / ((long long)RT * KF);
-    DevBuf<double> part;
-    HS_CUDA(part.alloc(2 * nflat));
-    RedArgs r1{Nn, nflat, N, RED_DOT, wM, wM, part.p, nullptr, nullptr};
-    k_reduce<<<(int)nflat, RT, 0, b->s>>>(r1);
-    k_final_reduce<<<1, RT, 0, b->s>>>(part.p, nflat, red.p);
-    RedArgs r2{Nn, nflat, N, RED_DOT, wA, wA, part.p, nullptr, nullptr};
-    k_reduce<<<(int)nflat, RT, 0, b->s>>>(r2);
-    k_final_reduce<<<1, RT, 0, b->s>>>(part.p, nflat, red.p + 2);
-    double nr[4];
-    HS_CUDA(cudaMemcpyAsync(nr, red.p, 4 * 8, cudaMemcpyDeviceToHost, b->s));
-    HS_CUDA(cudaStreamSynchronize(b->s));
+    if (!b->sq.p) HS_CUDA(b->sq.alloc(4));
+    if (b->spart.n < (size_t)(2 * nflat)) HS_CUDA(b->spart.alloc(2 * nflat));   // s_add is its only user
+    RedArgs r1{Nn, nflat, N, RED_DOT, wM, wM, b->spart.p, nullptr, nullptr};
+    k_reduce<<<(int)nflat, RT, 0, sa>>>(r1);
+    k_final_reduce<<<1, RT, 0, sa>>>(b->spart.p, nflat, b->sq.p);
+    RedArgs r2{Nn, nflat, N, RED_DOT, wA, wA, b->spart.p, nullptr, nullptr};
+    k_reduce<<<(int)nflat, RT, 0, sa>>>(r2);
+    k_final_reduce<<<1, RT, 0, sa>>>(b->spart.p, nflat, b->sq.p + 2);
+    kb_init_state<<<1, 1, 0, sa>>>(b->d_st.p + slot, b->sq.p);
     HS_CUDA(cudaGetLastError());
-    BState st0{};
-    st0.norm_wM = std::sqrt(nr[0]); st0.norm_wA = std::sqrt(nr[2]);
-    st0.odone = 1; st0.done = 1;
-    HS_CUDA(cudaMemcpyAsync(b->d_st.p + slot, &st0, sizeof(BState), cudaMemcpyHostToDevice, b->s));
-    HS_CUDA(cudaStreamSynchronize(b->s));
+    // the caller's host arrays are free again once this returns
+    HS_CUDA(cudaStreamSynchronize(sa));
     sl.used = true; sl.N = N; sl.dt = dt; sl.steps_left = n_steps; sl.steps_done = 0;
     sl.part = batch_part(N, b->opt.tile_planes);
     d.part = sl.part;
@@ -463,64 +476,85 @@ hs_status hs_batch_remove(hs_batch* b, int slot) {
         return HS_ERR_ARG;
     }
     HS_CUDA(cudaSetDevice(b->opt.device));
-    HS_CUDA(cudaStreamSynchronize(b->s));
     auto& sl = b->slots[slot];
-    cudaFree(sl.mem);
+    HS_CUDA(cudaFreeAsync(sl.mem, b->s));      // after every step already queued
     sl = hs_batch::Slot{};
+    sl.held = b->inflight;
     sl.desc.st = b->d_st.p + slot;
     b->dirty = true;
     return HS_OK;
 }
 
-hs_status hs_batch_step(hs_batch* b, int* n_active, double* device_ms) {
+hs_status hs_batch_step_begin(hs_batch* b, int* n_active) {
     if (!b) { set_error("bad arguments"); return HS_ERR_ARG; }
+    if (b->inflight) { set_error("hs_batch_step_begin: a step is already in flight"); return HS_ERR_ARG; }
     HS_CUDA(cudaSetDevice(b->opt.device));
     int act = 0;
-    for (auto& sl : b->slots) if (sl.used && sl.steps_left > 0) ++act;
+    for (auto& sl : b->slots) {
+        sl.in_step = sl.used && sl.steps_left > 0;
+        act += sl.in_step ? 1 : 0;
+    }
     if (n_active) *n_active = act;
-    if (device_ms) *device_ms = 0.0;
     if (act == 0) return HS_OK;
     // activity follows the steps left: refresh the descriptors when it changes
-    for (auto& sl : b->slots) if (sl.used && sl.desc.active != (sl.steps_left > 0 ? 1 : 0)) b->dirty = true;
+    for (auto& sl : b->slots) if (sl.used && sl.desc.active != (sl.in_step ? 1 : 0)) b->dirty = true;
     if (b->dirty) {
         hs_status st = upload(b);
         if (st != HS_OK) return st;
-        for (auto& sl : b->slots) sl.desc.active = (sl.used && sl.steps_left > 0) ? 1 : 0;
+        for (auto& sl : b->slots) sl.desc.active = sl.in_step ? 1 : 0;
     }
     const bool graph = graphs_enabled();
     hs_status st = graph ? build_batch_graph(b) : HS_OK;
     if (st != HS_OK) return st;
     // armed flips of this step (level G: one bit of the field before the step)
     for (auto& sl : b->slots) {
-        if (!sl.used || sl.steps_left <= 0) continue;
+        if (!sl.in_step) continue;
         if (sl.flip_step == sl.steps_done) k_flip<<<1, 1, 0, b->s>>>(sl.desc.T, sl.flip_idx, sl.flip_bit);
         if (sl.fault.level && sl.fault.step == sl.steps_done)
             kb_arm<<<1, 1, 0, b->s>>>(sl.desc.st, sl.fault.level, sl.fault.outer, sl.fault.iter, sl.fault.idx,
                                       sl.fault.bit);
     }
-    cudaEvent_t e0, e1;
-    HS_CUDA(cudaEventCreate(&e0));
-    HS_CUDA(cudaEventCreate(&e1));
-    HS_CUDA(cudaEventRecord(e0, b->s));
+    HS_CUDA(cudaEventRecord(b->ev0, b->s));
     if (graph) {
         HS_CUDA(cudaGraphLaunch(b->gexec, b->s));
     } else {
         st = step_direct(b);
         if (st != HS_OK) return st;
     }
-    HS_CUDA(cudaEventRecord(e1, b->s));
-    HS_CUDA(cudaEventSynchronize(e1));
-    HS_CUDA(cudaGetLastError());
-    for (auto& sl : b->slots)
-        if (sl.used && sl.steps_left > 0 && sl.fault.level && sl.fault.step == sl.steps_done)
-            kb_arm<<<1, 1, 0, b->s>>>(sl.desc.st, 0, 0, 0, 0, 0);
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0); cudaEventDestroy(e1);
-    if (device_ms) *device_ms = ms;
-    for (auto& sl : b->slots)
-        if (sl.used && sl.steps_left > 0) { --sl.steps_left; ++sl.steps_done; }
+    HS_CUDA(cudaEventRecord(b->ev1, b->s));
+    b->inflight = true;
     return HS_OK;
+}
+
+hs_status hs_batch_step_end(hs_batch* b, int* n_stepped, double* device_ms) {
+    if (!b) { set_error("bad arguments"); return HS_ERR_ARG; }
+    if (n_stepped) *n_stepped = 0;
+    if (device_ms) *device_ms = 0.0;
+    if (!b->inflight) return HS_OK;            // nothing was launched
+    HS_CUDA(cudaSetDevice(b->opt.device));
+    b->inflight = false;
+    HS_CUDA(cudaEventSynchronize(b->ev1));
+    HS_CUDA(cudaGetLastError());
+    int n = 0;
+    for (auto& sl : b->slots) {
+        sl.held = false;
+        if (!sl.in_step) continue;
+        if (sl.fault.level && sl.fault.step == sl.steps_done) kb_arm<<<1, 1, 0, b->s>>>(sl.desc.st, 0, 0, 0, 0, 0);
+        --sl.steps_left; ++sl.steps_done; ++n;
+        sl.in_step = false;
+    }
+    float ms = 0.f;
+    HS_CUDA(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+    if (n_stepped) *n_stepped = n;
+    if (device_ms) *device_ms = ms;
+    return HS_OK;
+}
+
+hs_status hs_batch_step(hs_batch* b, int* n_active, double* device_ms) {
+    if (device_ms) *device_ms = 0.0;
+    hs_status st = hs_batch_step_begin(b, n_active);
+    if (st != HS_OK) return st;
+    return hs_batch_step_end(b, nullptr, device_ms);
 }
 
 hs_status hs_batch_info(hs_batch* b, int slot, hs_batch_inst_info* out) {

@@ -591,6 +591,22 @@ __global__ void k_recip32(long long n, const double* d, float* out) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         out[i] = (float)__ddiv_rn(1.0, d[i]);
 }
+// interleaved FP64 and FP32 element coefficients (rho*c, k)
+__global__ void k_pack_coef(long long ne, const double* rhoc, const double* k, double2* c64, float2* c32) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < ne; i += (long long)gridDim.x * blockDim.x) {
+        const double r = rhoc[i], kk = k[i];
+        c64[i] = make_double2(r, kk);
+        c32[i] = make_float2(__double2float_rn(r), __double2float_rn(kk));
+    }
+}
+// fresh state of an added instance: checksum weight norms from their squared sums, nothing to iterate
+__global__ void kb_init_state(BState* st, const double* sq) {
+    BState s{};
+    s.norm_wM = __dsqrt_rn(sq[0]);
+    s.norm_wA = __dsqrt_rn(sq[2]);
+    s.odone = 1; s.done = 1;
+    *st = s;
+}
 __global__ void k_ones_interior(int N, double* v) {
     const long long NN = N + 1, Nn = NN * NN * NN;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < Nn; i += (long long)gridDim.x * blockDim.x)

@@ -211,7 +211,9 @@ def serving(n=400, rate=200.0, seed=11, rtol=1e-8, inner_tol=1e-4, max_live=64, 
     lat, live, queue = {}, {}, list(reqs)
     live_bytes, peak_live = 0, 0
     t0 = time.perf_counter()
-    while queue or live:
+
+    def admit():
+        nonlocal live_bytes
         now = time.perf_counter() - t0
         while (queue and queue[0]["t"] <= now and len(live) < max_live and
                live_bytes + batch_bytes(queue[0]["N"]) <= budget):
@@ -222,15 +224,24 @@ def serving(n=400, rate=200.0, seed=11, rtol=1e-8, inner_tol=1e-4, max_live=64, 
                 b.arm_flip(s, *q["flip"])
             q["left"] = q["steps"]
             live[s] = q
-        peak_live = max(peak_live, len(live))
+
+    while queue or live:
         if not live:
-            time.sleep(max(0.0, queue[0]["t"] - (time.perf_counter() - t0)))
+            admit()
+            if not live:
+                time.sleep(max(0.0, queue[0]["t"] - (time.perf_counter() - t0)))
             continue
-        b.step()
+        # the live instances step on the GPU while the host sets up arrivals;
+        # those join at the next step
+        stepping = list(live)
+        b.step_begin()
+        admit()
+        b.step_end()
+        peak_live = max(peak_live, len(live))
         done_at = time.perf_counter() - t0
-        for q in live.values():
-            q["left"] -= 1
-        for s in [s for s, q in live.items() if q["left"] == 0]:
+        for s in stepping:
+            live[s]["left"] -= 1
+        for s in [s for s in stepping if live[s]["left"] == 0]:
             q = live.pop(s)
             live_bytes -= batch_bytes(q["N"])
             lat[q["id"]] = done_at - q["t"]

@@ -94,6 +94,42 @@ def test_join_running_batch_and_reuse_slot(oracle):
     b.close()
 
 
+def test_admission_during_a_step_in_flight(oracle):
+    """hs_batch_step_begin / _end: instances added while a step runs join at
+    the next step, a slot removed during a step is not reused before it ends,
+    and every instance gives the bits of its solo run."""
+    (N1, dt1, st1, sd1), (N2, dt2, st2, sd2), (N3, dt3, st3, sd3) = CASES[1], CASES[0], CASES[2]
+    ref1, ref2, ref3 = (_solo(oracle, *CASES[1])[0], _solo(oracle, *CASES[0])[0], _solo(oracle, *CASES[2])[0])
+    b = _lib.Batch(rtol=1e-8)
+    k, r = field(N1, "lognormal", sigma=1.0, L=0.25, seed=sd1)
+    a = b.add(N1, dt1, k, r, T0=gaussian_T0(oracle, N1, dt1, k, r), steps=st1)
+    k, r = field(N2, "lognormal", sigma=1.0, L=0.25, seed=sd2)
+    c = b.add(N2, dt2, k, r, T0=gaussian_T0(oracle, N2, dt2, k, r), steps=st2)
+    assert b.step_begin() == 2
+    with pytest.raises(_lib.HeatError):
+        b.step_begin()                                  # one step in flight at a time
+    k, r = field(N3, "lognormal", sigma=1.0, L=0.25, seed=sd3)
+    d = b.add(N3, dt3, k, r, T0=gaussian_T0(oracle, N3, dt3, k, r), steps=st3)   # set up beside the step
+    assert b.step_end()[0] == 2                         # d was not part of it
+    assert b.info(d)["steps_done"] == 0 and b.info(a)["steps_done"] == 1
+    while b.info(c)["steps_left"] > 0:
+        b.step_begin()
+        b.step_end()
+    assert np.array_equal(bits(b.field(c)), bits(ref2))
+    b.step_begin()
+    b.remove(c)                                         # freed after the step; its slot is held
+    e = b.add(N2, dt2, np.ones(N2 ** 3), np.ones(N2 ** 3), steps=1)
+    assert e not in (a, c, d)
+    b.step_end()
+    b.remove(e)
+    while b.step()[0]:
+        pass
+    assert np.array_equal(bits(b.field(a)), bits(ref1))
+    assert np.array_equal(bits(b.field(d)), bits(ref3))
+    assert b.step_end() == (0, 0.0)                     # nothing in flight
+    b.close()
+
+
 def test_tile_depth_changes_only_rounding(oracle):
     T1, _ = _solo(oracle, 20, 2e-4, 3, 3, planes=0)
     T4, _ = _solo(oracle, 20, 2e-4, 3, 3, planes=5)
