@@ -323,10 +323,11 @@ def main():
     traffic = profile_traffic(N)
     iters_per_traj = it_all / max(1, world) / args.steps
     # per time step: step begin/end, RHS and x0 operator (+ final each with ABFT),
-    # PCG prologue (update + final); per CG iteration: operator + final,
-    # update + final
+    # PCG prologue (update + final); per CG iteration: operator, update (which
+    # finishes the operator's reductions) + final; the atomic scatter adds
+    # p formation, zeroing and the finishing pass to the operator
     per_step = (2 + 2 * (2 if detect else 1) + 2) if args.scatter == "colored" else 12
-    per_iter = 4 if args.scatter == "colored" else 6
+    per_iter = 3 if args.scatter == "colored" else 6
     launches = int(round(args.steps * (STEPS_PER_TRAJ * per_step + per_iter * iters_per_traj)))
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,

@@ -260,9 +260,8 @@ __device__ __forceinline__ void store_partials(double (&v)[NQ], double* partials
 // The strided sums take their partials in batches of FB per quantity: all the
 // batch's loads are issued before the (in-order) adds, so the pass costs a
 // few memory latencies instead of one per partial.
-template <int NQ>
+template <int NQ, int FB = 16>
 __device__ __forceinline__ void final_sums(double (&v)[NQ], const double* partials, long long nblk, double (*sh)[8]) {
-    constexpr int FB = 16;
 #pragma unroll
     for (int q = 0; q < NQ; ++q) v[q] = 0.0;
     for (long long k0 = threadIdx.x; k0 < nblk; k0 += (long long)RT * FB) {
@@ -566,16 +565,23 @@ struct UpdateArgs {
     unsigned* ticket;
     DevState* st;
     cudaGraphConditionalHandle cond;
-    int use_cond, pad;
+    int use_cond, d1;           // d1: the loop operator's checksum is evaluated (CTA 0)
+    const double* apart;        // LOOP: the operator's tile partials (p.Ap, 1_int.Ap, w.p, p.p)
+    long long nblk;             // LOOP: their count per quantity
 };
 
 // PCG vector update on the flat partition: each thread updates its KF
 // consecutive nodes (KF / 2 aligned 128-bit loads and stores per vector), in
-// order.
-__global__ void __launch_bounds__(RT, KF <= 2 ? 6 : (KF <= 4 ? 4 : 2)) k_update(UpdateArgs a) {
+// order.  In the loop it also finishes the operator's reductions: every CTA
+// sums p.Ap over the tile partials in the canonical order (so alpha = rho /
+// p.Ap is the same bits everywhere), and CTA 0 records p.Ap, alpha, the D1
+// checksum and a breakdown, the work a separate single-CTA kernel would do.
+constexpr int kUpdateCtasPerSm = 5;
+__global__ void __launch_bounds__(RT, kUpdateCtasPerSm) k_update(UpdateArgs a) {
     static_assert(KF % 2 == 0, "pairs of nodes per thread");
     constexpr int NC = KF / 2;
     __shared__ double sh[MAXQ][8];
+    __shared__ double s_pAp;
     DevState* st = a.st;
     const int tid = threadIdx.x;
     if (a.role == UPD_LOOP && st->done) return;
@@ -586,67 +592,100 @@ __global__ void __launch_bounds__(RT, KF <= 2 ? 6 : (KF <= 4 ? 4 : 2)) k_update(
     int fi_r = 0, fi_bit = 0;
     long long fi_idx = -1;
     if (!pre) {
-        iter = st->iter; alpha = st->alpha;
+        iter = st->iter;
         p = (iter & 1) ? a.pbuf1 : a.pbuf0;
         if (st->fi_vec == FI_RV && st->fi_iter == iter) { fi_r = 1; fi_idx = st->fi_idx; fi_bit = st->fi_bit; }
+        // alpha from the operator's partials, once per CTA (short load batches keep the registers low)
+        if (blockIdx.x == 0) {
+            double q[MAXQ];
+            final_sums<MAXQ, 2>(q, a.apart, a.nblk, sh);
+            if (tid == 0) {
+                if (a.d1) {
+                    const double nx = __dsqrt_rn(q[3]);
+                    double rel = __ddiv_rn(fabs(dsub(q[1], q[2])), dfma(st->norm_wA, nx, 1e-300));
+                    if (!isfinite(rel)) rel = 1e300;
+                    st->d1_last = rel;
+                    st->d1_step = fmax(st->d1_step, rel);
+                }
+                st->pAp = q[0];
+                if (fabs(q[0]) < 1e-30) { st->broken = 1; st->done = 1; st->result = st->iter; }
+                else st->alpha = __ddiv_rn(st->rho, q[0]);
+                s_pAp = q[0];
+            }
+        } else {
+            double q[1];
+            final_sums<1, 8>(q, a.apart, a.nblk, sh);
+            if (tid == 0) s_pAp = q[0];
+        }
+        __syncthreads();
+        const double pAp = s_pAp;
+        if (fabs(pAp) < 1e-30) return;          // breakdown: the reference stops before the update
+        alpha = __ddiv_rn(st->rho, pAp);
     }
     const double nalpha = -alpha;
-    double part[3] = {0.0, 0.0, 0.0};   // PRE: bb, rz, rr   LOOP: rr, rz, -
-    const long long m0 = ((long long)blockIdx.x * RT + tid) * KF;
-    int cnt[NC];
-#pragma unroll
-    for (int c = 0; c < NC; ++c) {
-        const long long m = m0 + 2 * c;
-        cnt[c] = (m + 1 < a.Nn) ? 2 : (m < a.Nn ? 1 : 0);
-    }
-    auto ld = [&](const double* base, double (&v)[KF]) {
+    // flat blocks blockIdx.x, + gridDim.x, ...; each block's partials at its own index
+    for (long long blk = blockIdx.x; blk < a.nflat; blk += gridDim.x) {
+        double part[3] = {0.0, 0.0, 0.0};   // PRE: bb, rz, rr   LOOP: rr, rz, -
+        const long long m0 = (blk * RT + tid) * KF;
+        int cnt[NC];
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
             const long long m = m0 + 2 * c;
-            if (cnt[c] == 2) { const double2 t = __ldg(reinterpret_cast<const double2*>(base + m)); v[2 * c] = t.x; v[2 * c + 1] = t.y; }
-            else { v[2 * c] = cnt[c] ? __ldg(base + m) : 0.0; v[2 * c + 1] = 0.0; }
+            cnt[c] = (m + 1 < a.Nn) ? 2 : (m < a.Nn ? 1 : 0);
         }
-    };
-    auto stv = [&](double* base, const double (&v)[KF]) {
+        auto ld = [&](const double* base, double (&v)[KF]) {
 #pragma unroll
-        for (int c = 0; c < NC; ++c) {
-            const long long m = m0 + 2 * c;
-            if (cnt[c] == 2) *reinterpret_cast<double2*>(base + m) = make_double2(v[2 * c], v[2 * c + 1]);
-            else if (cnt[c] == 1) base[m] = v[2 * c];
-        }
-    };
-    auto has = [&](int k) { return k % 2 < cnt[k / 2]; };
-    if (pre) {
-        double bb[KF], qq[KF], dd[KF], r_[KF], z_[KF];
-        ld(a.b, bb); ld(a.Ap, qq); ld(a.d, dd);
+            for (int c = 0; c < NC; ++c) {
+                const long long m = m0 + 2 * c;
+                if (cnt[c] == 2) { const double2 t = __ldg(reinterpret_cast<const double2*>(base + m)); v[2 * c] = t.x; v[2 * c + 1] = t.y; }
+                else { v[2 * c] = cnt[c] ? __ldg(base + m) : 0.0; v[2 * c + 1] = 0.0; }
+            }
+        };
+        auto stv = [&](double* base, const double (&v)[KF]) {
 #pragma unroll
-        for (int k = 0; k < KF; ++k) {
-            r_[k] = 0.0; z_[k] = 0.0;
-            if (!has(k)) continue;
-            r_[k] = dfma(-1.0, qq[k], bb[k]);
-            z_[k] = __ddiv_rn(r_[k], dd[k]);
-            part[0] = dfma(bb[k], bb[k], part[0]);
-            part[1] = dfma(r_[k], z_[k], part[1]);
-            part[2] = dfma(r_[k], r_[k], part[2]);
-        }
-        stv(a.r, r_); stv(a.z, z_);
-    } else {
-        double xx[KF], pp[KF], qq[KF], rr[KF], dd[KF];
-        ld(a.x, xx); ld(p, pp); ld(a.Ap, qq); ld(a.r, rr); ld(a.d, dd);
+            for (int c = 0; c < NC; ++c) {
+                const long long m = m0 + 2 * c;
+                if (cnt[c] == 2) *reinterpret_cast<double2*>(base + m) = make_double2(v[2 * c], v[2 * c + 1]);
+                else if (cnt[c] == 1) base[m] = v[2 * c];
+            }
+        };
+        auto has = [&](int k) { return k % 2 < cnt[k / 2]; };
+        if (pre) {
+            double bb[KF], qq[KF], dd[KF], r_[KF], z_[KF];
+            ld(a.b, bb); ld(a.Ap, qq); ld(a.d, dd);
 #pragma unroll
-        for (int k = 0; k < KF; ++k) {
-            if (!has(k)) continue;
-            xx[k] = dfma(alpha, pp[k], xx[k]);
-            double rk = dfma(nalpha, qq[k], rr[k]);
-            if (fi_r && m0 + k == fi_idx) rk = flipbit(rk, fi_bit);
-            rr[k] = rk;
-            dd[k] = __ddiv_rn(rk, dd[k]);          // z
-            part[0] = dfma(rk, rk, part[0]);
-            part[1] = dfma(rk, dd[k], part[1]);
+            for (int k = 0; k < KF; ++k) {
+                r_[k] = 0.0; z_[k] = 0.0;
+                if (!has(k)) continue;
+                r_[k] = dfma(-1.0, qq[k], bb[k]);
+                z_[k] = __ddiv_rn(r_[k], dd[k]);
+                part[0] = dfma(bb[k], bb[k], part[0]);
+                part[1] = dfma(r_[k], z_[k], part[1]);
+                part[2] = dfma(r_[k], r_[k], part[2]);
+            }
+            stv(a.r, r_); stv(a.z, z_);
+        } else {
+            double xx[KF], pp[KF], qq[KF], rr[KF], dd[KF];
+            ld(a.x, xx); ld(p, pp); ld(a.Ap, qq); ld(a.r, rr); ld(a.d, dd);
+#pragma unroll
+            for (int k = 0; k < KF; ++k) {
+                if (!has(k)) continue;
+                xx[k] = dfma(alpha, pp[k], xx[k]);
+                double rk = dfma(nalpha, qq[k], rr[k]);
+                if (fi_r && m0 + k == fi_idx) rk = flipbit(rk, fi_bit);
+                rr[k] = rk;
+                dd[k] = __ddiv_rn(rk, dd[k]);          // z
+                part[0] = dfma(rk, rk, part[0]);
+                part[1] = dfma(rk, dd[k], part[1]);
+            }
+            stv(a.x, xx); stv(a.r, rr); stv(a.z, dd);
         }
-        stv(a.x, xx); stv(a.r, rr); stv(a.z, dd);
+        cta_tree_sum<3>(part, sh);
+        if (tid == 0) {
+#pragma unroll
+            for (int q = 0; q < 3; ++q) a.partials[q * a.nflat + blk] = part[q];
+        }
     }
-    store_partials<3>(part, a.partials, a.nflat, sh);
 }
 
 // PCG scalar logic after the vector update: the prologue's ||b||, rho and

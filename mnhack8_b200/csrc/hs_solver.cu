@@ -69,7 +69,9 @@ struct hs_solver {
     DevBuf<double2> coef;               // (rho*c, k) per element, the operator kernel's layout
     DevBuf<double> diag, F, wM, wA;
     DevBuf<double> T, b, r, z, p0, p1, Ap;
-    DevBuf<double> partials;
+    DevBuf<double> partials;            // operator tiles (and the standalone reductions)
+    DevBuf<double> upart;               // PCG vector update blocks (read by the update's final kernel)
+    int n_sm = 148;
     DevBuf<unsigned> ticket;
     DevBuf<DevState> st;
     DevBuf<double> red;                 // standalone reduction outputs
@@ -180,8 +182,9 @@ void apply_projected(hs_solver* h, int role, const double* x, double* y, double 
         a.d1 = d1 ? 1 : 0;
         a.partials = h->partials.p; a.st = h->st.p; a.ec = h->ec;
         launch_colored(h, a);
-        if (role == ROLE_LOOP || d1) {
-            FinalApplyArgs fa{h->partials.p, h->part.nblk, h->st.p, role, d1 ? 1 : 0};
+        // the loop role's reductions are finished by the vector update (k_update)
+        if (role != ROLE_LOOP && d1) {
+            FinalApplyArgs fa{h->partials.p, h->part.nblk, h->st.p, role, 1};
             k_final_apply<<<1, RT, 0, h->s>>>(fa);
         }
         return;
@@ -201,8 +204,8 @@ void apply_projected(hs_solver* h, int role, const double* x, double* y, double 
     f.y = y; f.w = w; f.F = F; f.dtF = dtF;
     f.partials = h->partials.p; f.ticket = h->ticket.p; f.st = h->st.p;
     k_finish_atomic<<<nblocks(h), ST, 0, h->s>>>(f);
-    if (role == ROLE_LOOP || d1) {
-        FinalApplyArgs fa{h->partials.p, h->part.nblk, h->st.p, role, d1 ? 1 : 0};
+    if (role != ROLE_LOOP && d1) {
+        FinalApplyArgs fa{h->partials.p, h->part.nblk, h->st.p, role, 1};
         k_final_apply<<<1, RT, 0, h->s>>>(fa);
     }
 }
@@ -210,10 +213,13 @@ void apply_projected(hs_solver* h, int role, const double* x, double* y, double 
 void launch_update(hs_solver* h, int role, bool use_cond, cudaGraphConditionalHandle cond = 0) {
     UpdateArgs u{};
     u.Nn = h->Nn; u.nflat = h->part.nflat; u.role = role; u.x = h->T.p; u.b = h->b.p; u.r = h->r.p; u.z = h->z.p; u.Ap = h->Ap.p;
-    u.d = h->diag.p; u.pbuf0 = h->p0.p; u.pbuf1 = h->p1.p; u.partials = h->partials.p; u.ticket = h->ticket.p;
+    u.d = h->diag.p; u.pbuf0 = h->p0.p; u.pbuf1 = h->p1.p; u.partials = h->upart.p; u.ticket = h->ticket.p;
     u.st = h->st.p; u.cond = cond; u.use_cond = 0;
-    k_update<<<(int)h->part.nflat, RT, 0, h->s>>>(u);
-    FinalUpdateArgs fu{h->partials.p, h->part.nflat, h->st.p, cond, role, use_cond ? 1 : 0};
+    u.d1 = h->opt.detect != 0; u.apart = h->partials.p; u.nblk = h->part.nblk;
+    // one resident wave: the loop role sums the operator's partials once per CTA
+    const long long wave = (long long)h->n_sm * kUpdateCtasPerSm;
+    k_update<<<(int)std::min<long long>(h->part.nflat, wave), RT, 0, h->s>>>(u);
+    FinalUpdateArgs fu{h->upart.p, h->part.nflat, h->st.p, cond, role, use_cond ? 1 : 0};
     k_final_update<<<1, RT, 0, h->s>>>(fu);
 }
 
@@ -419,12 +425,16 @@ hs_status hs_create(const hs_options* opt, const double* k_host, const double* r
     h->ec.detJ = h->mats.detJ;
 
     HS_CUDA(cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking));
+    int dev = 0;
+    HS_CUDA(cudaGetDevice(&dev));
+    HS_CUDA(cudaDeviceGetAttribute(&h->n_sm, cudaDevAttrMultiProcessorCount, dev));
     const size_t Nn = (size_t)h->Nn, Ne = (size_t)h->Ne;
     HS_CUDA(h->rhoc.alloc(Ne)); HS_CUDA(h->kc.alloc(Ne)); HS_CUDA(h->gtab.alloc(256)); HS_CUDA(h->coef.alloc(Ne));
     HS_CUDA(h->diag.alloc(Nn)); HS_CUDA(h->F.alloc(Nn));
     HS_CUDA(h->T.alloc(Nn)); HS_CUDA(h->b.alloc(Nn)); HS_CUDA(h->r.alloc(Nn)); HS_CUDA(h->z.alloc(Nn));
     HS_CUDA(h->p0.alloc(Nn)); HS_CUDA(h->p1.alloc(Nn)); HS_CUDA(h->Ap.alloc(Nn));
     HS_CUDA(h->partials.alloc((size_t)MAXQ * std::max(h->part.nblk, h->part.nflat) + 4096));
+    HS_CUDA(h->upart.alloc((size_t)3 * h->part.nflat + 256));
     HS_CUDA(h->ticket.alloc(1)); HS_CUDA(h->st.alloc(1)); HS_CUDA(h->red.alloc(8)); HS_CUDA(h->sp.alloc(2));
     HS_CUDA(cudaMemsetAsync(h->ticket.p, 0, sizeof(unsigned), h->s));
     HS_CUDA(cudaMemsetAsync(h->st.p, 0, sizeof(DevState), h->s));
@@ -1034,6 +1044,8 @@ hs_status hs_time_kernel(hs_solver* h, int which, int reps, double* ms_per_launc
     std::vector<cudaEvent_t> ev(2 * (size_t)reps);
     for (auto& e : ev) HS_CUDA(cudaEventCreate(&e));
     const bool det = h->opt.detect != 0;
+    // the update finishes the operator's reductions: give it one operator's partials
+    if (which == 1) apply_projected(h, ROLE_LOOP, nullptr, h->Ap.p, h->opt.dt, det, h->wA.p, nullptr, 0.0);
     for (int r = 0; r < reps; ++r) {
         k_l2_scrub<<<148 * 8, 256, 0, h->s>>>(flush.p, (long long)fl, h->red.p + 5);
         HS_CUDA(cudaEventRecord(ev[2 * r], h->s));
