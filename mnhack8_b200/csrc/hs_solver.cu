@@ -253,7 +253,11 @@ bool graphs_enabled() {
     return v == 1;
 }
 
-// build a graph: [rhs] + x0 matvec + prologue, then while(!done){ K1; K2 }
+// build a graph: [rhs] + x0 matvec + prologue, then while(!done){ (K1; K2) x kLoopUnroll }.
+// Four iterations per pass of the while body spread the node's relaunch over
+// them (N=128: 70.6 -> 67.8 us per CG iteration); a solve that ends mid-pass
+// launches at most three iterations' kernels that return at once.
+constexpr int kLoopUnroll = 4;
 hs_status build_graph(hs_solver* h, int which) {
     if (h->gexec[which] || !graphs_enabled()) return HS_OK;
     const bool with_rhs = which == 0;
@@ -278,8 +282,12 @@ hs_status build_graph(hs_solver* h, int which) {
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     HS_CUDA(cudaStreamBeginCaptureToGraph(h->s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     const bool det = h->opt.detect != 0;
-    apply_projected(h, ROLE_LOOP, nullptr, h->Ap.p, h->opt.dt, det, h->wA.p, nullptr, 0.0);
-    launch_update(h, UPD_LOOP, true, cond);
+    // kLoopUnroll iterations per pass of the while body: every kernel returns at
+    // once when the solve is done, and each final kernel sets the condition
+    for (int u = 0; u < kLoopUnroll; ++u) {
+        apply_projected(h, ROLE_LOOP, nullptr, h->Ap.p, h->opt.dt, det, h->wA.p, nullptr, 0.0);
+        launch_update(h, UPD_LOOP, true, cond);
+    }
     HS_CUDA(cudaStreamEndCapture(h->s, &body));
     HS_CUDA(cudaGraphInstantiate(&h->gexec[which], g, 0));
     h->graph[which] = g;
