@@ -229,10 +229,13 @@ hs_status build_batch_graph(hs_batch* b) {
     HS_CUDA(cudaGraphAddNode(&n_in, obody, &n_head, 1, &pi));
     cudaGraph_t ibody = pi.conditional.phGraph_out[0];
     HS_CUDA(cudaStreamBeginCaptureToGraph(b->s, ibody, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    kb_apply<float, BK_LOOP><<<(int)a.ntiles, ST, sizeof(BSlabSmem<float>), b->s>>>(a);
-    kb_final_apply<BK_LOOP><<<a.n_inst, RT, 0, b->s>>>(a);
-    kb_update32<<<(int)a.nflat, RT, 0, b->s>>>(a);
-    kb_final_update32<<<a.n_inst, RT, 0, b->s>>>(a);
+    // four inner iterations per pass (an instance that is done skips them), one condition
+    for (int u = 0; u < 4; ++u) {
+        kb_apply<float, BK_LOOP><<<(int)a.ntiles, ST, sizeof(BSlabSmem<float>), b->s>>>(a);
+        kb_final_apply<BK_LOOP><<<a.n_inst, RT, 0, b->s>>>(a);
+        kb_update32<<<(int)a.nflat, RT, 0, b->s>>>(a);
+        kb_final_update32<<<a.n_inst, RT, 0, b->s>>>(a);
+    }
     kb_cond<1><<<1, 1024, 0, b->s>>>(a, c_in, nullptr);
     HS_CUDA(cudaStreamEndCapture(b->s, &ibody));
     cudaGraph_t otail;
