@@ -513,9 +513,9 @@ __global__ void __launch_bounds__(ST, FORM == FORM_WHT ? 2 : 1) k_apply_slab(App
     store_partials<MAXQ>(part, a.partials, a.part.nblk, S.sh);
 }
 
-// Role logic of an operator application once its partials are complete:
-// the D1 checksum (relative mismatch of 1_int.(Ax) and w.x) and, in the PCG
-// loop, alpha = rho / p.Ap (or the reference's breakdown exit).
+// The D1 checksum (relative mismatch of 1_int.(Ax) and w.x) of an operator
+// application outside the PCG loop, once its partials are complete.  The loop
+// role's reductions (p.Ap, alpha, D1, breakdown) are finished by k_update.
 struct FinalApplyArgs {
     const double* partials;
     long long nblk;
@@ -525,28 +525,15 @@ struct FinalApplyArgs {
 __global__ void __launch_bounds__(RT) k_final_apply(FinalApplyArgs a) {
     __shared__ double sh[MAXQ][8];
     DevState* st = a.st;
-    const bool loop = a.role == ROLE_LOOP;
-    if (loop && st->done) return;
     double part[MAXQ];
     final_sums<MAXQ>(part, a.partials, a.nblk, sh);
-    if (threadIdx.x != 0) return;
-    if (a.d1) {
-        const double nw = (a.role == ROLE_RHS) ? st->norm_wM : st->norm_wA;
-        const double nx = __dsqrt_rn(part[3]);
-        double rel = __ddiv_rn(fabs(dsub(part[1], part[2])), dfma(nw, nx, 1e-300));
-        if (!isfinite(rel)) rel = 1e300;
-        st->d1_last = rel;
-        if (a.role != ROLE_USER) st->d1_step = fmax(st->d1_step, rel);
-    }
-    if (loop) {
-        const double pAp = part[0];
-        st->pAp = pAp;
-        if (fabs(pAp) < 1e-30) {
-            st->broken = 1; st->done = 1; st->result = st->iter;
-        } else {
-            st->alpha = __ddiv_rn(st->rho, pAp);
-        }
-    }
+    if (threadIdx.x != 0 || !a.d1) return;
+    const double nw = (a.role == ROLE_RHS) ? st->norm_wM : st->norm_wA;
+    const double nx = __dsqrt_rn(part[3]);
+    double rel = __ddiv_rn(fabs(dsub(part[1], part[2])), dfma(nw, nx, 1e-300));
+    if (!isfinite(rel)) rel = 1e300;
+    st->d1_last = rel;
+    if (a.role != ROLE_USER) st->d1_step = fmax(st->d1_step, rel);
 }
 
 // ---- PCG vector update (canonical partition) -----------------------------------
