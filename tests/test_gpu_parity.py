@@ -107,6 +107,25 @@ def test_build_rhs_and_pcg_bitwise(oracle, dev, form, N):
     g.close()
 
 
+@pytest.mark.parametrize("max_iter", [1, 2, 5, 6, 7, 9])
+def test_pcg_iteration_cap_bitwise(oracle, dev, max_iter):
+    """The CUDA graph runs several CG iterations per pass of its while body; a solve
+    stopped by the iteration cap in the middle of a pass ends with the oracle's
+    iterate and count."""
+    N = 17
+    k, r = field(N, "lognormal", sigma=1.0, L=0.25, seed=5)
+    o = oracle.Oracle(N, 5e-4, k, r, form="wht", detect=True, ic="gaussian", ic_sigma=0.15)
+    g = _lib.Solver(N, 5e-4, k, r, kernel="wht", scatter="colored", detect=True, ic="gaussian", ic_sigma=0.15)
+    T = o.initial_condition()
+    b_ref = o.build_rhs(T)
+    bd, xd = dev.put(b_ref), dev.put(T)
+    it = g.pcg_ptr(bd.data_ptr(), xd.data_ptr(), max_iter, 1e-14)
+    it_ref, x_ref, _ = o.pcg(b_ref, T, max_iter, 1e-14)
+    assert it == it_ref == max_iter
+    assert np.array_equal(bits(dev.get(xd)), bits(x_ref))
+    g.close()
+
+
 def _cmp_records(got, want, E=True):
     for s, (a, b) in enumerate(zip(got["steps"], want["steps"])):
         assert a["cg_iters"] == b["cg_iters"], s
