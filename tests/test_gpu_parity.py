@@ -65,6 +65,47 @@ def test_apply_bitwise_split_tiles(oracle, dev, N):
     g.close()
 
 
+@pytest.mark.parametrize("N", [128, 256])
+def test_apply_bitwise_at_workload_sizes(oracle, dev, N):
+    """The operator at the sizes the measurements use (the bench trajectory,
+    N=128, and the precision configuration, N=256), on the bench's own seeded
+    lognormal field: every value and the checksum bit for bit."""
+    import bench
+
+    k, r = bench.make_field(N, 1)
+    o = oracle.Oracle(N, 1e-4, k, r, form="wht", colored=True, detect=True)
+    g = _lib.Solver(N, 1e-4, k, r, kernel="wht", scatter="colored", detect=True)
+    x = random_nodes(N, 300 + N)
+    xd, yd = dev.put(x), dev.zeros(o.Nn)
+    rel = g.apply_ptr(xd.data_ptr(), yd.data_ptr(), dt_eff=o.dt, project=True)
+    y_ref, rel_ref = o.apply(x, dt_eff=o.dt, project=True, d1=True)
+    assert np.array_equal(bits(dev.get(yd)), bits(y_ref))
+    assert np.float64(rel).view(np.uint64) == np.float64(rel_ref).view(np.uint64)
+    g.close()
+
+
+def test_operator_symmetry_and_linearity_N256(dev):
+    """Size-independent properties at N=256: on interior vectors the projected
+    operator is symmetric (x.Ay = y.Ax to rounding) and linear
+    (A(x + 2y) = Ax + 2Ay to rounding)."""
+    import bench
+
+    N = 256
+    k, r = bench.make_field(N, 2)
+    g = _lib.Solver(N, 1e-4, k, r, kernel="wht", scatter="colored", detect=True)
+    x, y = random_nodes(N, 11, boundary=False), random_nodes(N, 12, boundary=False)
+    xd, yd, zd = dev.put(x), dev.put(y), dev.put(x + 2.0 * y)
+    ax, ay, az = dev.zeros(x.size), dev.zeros(x.size), dev.zeros(x.size)
+    for src, dst in ((xd, ax), (yd, ay), (zd, az)):
+        g.apply_ptr(src.data_ptr(), dst.data_ptr(), project=True)
+    Ax, Ay, Az = dev.get(ax), dev.get(ay), dev.get(az)
+    g.close()
+    xAy, yAx = float(np.dot(x, Ay)), float(np.dot(y, Ax))
+    assert abs(xAy - yAx) <= 1e-12 * max(abs(xAy), np.linalg.norm(x) * np.linalg.norm(Ay))
+    lin = Ax + 2.0 * Ay
+    assert np.linalg.norm(Az - lin) <= 1e-14 * np.linalg.norm(lin) * 8
+
+
 def test_apply_rejects_overlap(oracle, dev):
     o, g = pair(oracle, 8, "wht")
     xd = dev.put(random_nodes(8, 1))
