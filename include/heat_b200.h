@@ -296,14 +296,16 @@ hs_status hs_batch_get_field(hs_batch* b, int slot, double* T_host);
  * call cudaMalloc (a host application that owns the device-memory budget, a
  * path that must not take the allocator's locks): the result equals hs_dot's
  * bit for bit (same fixed reduction order), but the per-block partial sums
- * live in a static device array of 65536 doubles (512 KiB, held by every GPU
- * that loads the library until exit), so N <= 321 ((N+1)^3 <= 33554432 nodes);
- * larger grids return HS_ERR_ARG.  x, y and out (one double) are device
- * pointers on the current device; the work is enqueued on the default stream
- * and *out is valid once that stream has completed.  The first call on a
- * device looks up the array's device address and should come before any
- * stream capture.  All calls share the array: calls that overlap on the GPU
- * race. */
+ * live in a static device array of 131072 doubles (1 MiB, held by every GPU
+ * that loads the library until exit).  The reduction stores two values per
+ * block of 512 nodes, so the array serves 65536 blocks: N <= 321; larger
+ * grids return HS_ERR_ARG before anything is launched.  x, y and out (one
+ * double) are device pointers on the current device; the work is enqueued on
+ * the default stream and *out is valid once that stream has completed.  The
+ * first call on a device looks up the array's device address and should come
+ * before any stream capture.  All calls share the array: calls that overlap
+ * on the GPU race.  Do not call it on a device after cudaDeviceReset (the
+ * cached address of the array is then stale). */
 hs_status hs_dot_noalloc(int N, const double* x, const double* y, double* out);
 
 /* The reference solver's command line (het.cu:1340-1350, 1380-1433) with its

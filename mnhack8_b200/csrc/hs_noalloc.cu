@@ -20,10 +20,14 @@
 
 namespace hs {
 
-// Partial sums of the flat reduction order (one per block of RT*KF nodes).
-// Every GPU that loads the library holds this array (512 KiB) until exit.
-constexpr long long kNoAllocMaxPartials = 65536;
-static __device__ __align__(256) double g_noalloc_partials[kNoAllocMaxPartials];
+// Partial sums of the flat reduction order.  k_reduce stores two quantities
+// per block of RT*KF nodes (partials[q*nflat + block], q = 0, 1; a dot uses
+// only q = 0 but the slot of q = 1 is written all the same), so a grid of
+// nflat blocks needs 2*nflat doubles.  Every GPU that loads the library holds
+// this array (1 MiB) until exit.
+constexpr long long kNoAllocMaxBlocks = 65536;                 // nflat limit: N <= 321
+constexpr long long kNoAllocPartials = 2 * kNoAllocMaxBlocks;  // doubles in the array
+static __device__ __align__(256) double g_noalloc_partials[kNoAllocPartials];
 
 // final combination of the partials into *out (one value)
 __global__ void __launch_bounds__(RT) k_final_dot_noalloc(long long nflat, double* out) {
@@ -35,7 +39,10 @@ __global__ void __launch_bounds__(RT) k_final_dot_noalloc(long long nflat, doubl
 
 namespace {
 std::mutex g_mu;
-double* g_addr[128] = {nullptr};   // host-usable device address of the array, per device
+// Host-usable device address of the array, per device, looked up once.  A
+// cudaDeviceReset unloads the module, after which the cached address is
+// stale: do not call hs_dot_noalloc on a device after resetting it.
+double* g_addr[128] = {nullptr};
 }  // namespace
 
 }  // namespace hs
@@ -45,14 +52,19 @@ extern "C" hs_status hs_dot_noalloc(int N, const double* x, const double* y, dou
     if (N < 1 || N > 1200 || !x || !y || !out) { set_error("hs_dot_noalloc: bad arguments"); return HS_ERR_ARG; }
     const long long NN = N + 1, Nn = NN * NN * NN;
     const long long nflat = (Nn + (long long)RT * KF - 1) / ((long long)RT * KF);
-    if (nflat > kNoAllocMaxPartials) {
-        set_error("hs_dot_noalloc: grid too large for the static scratch (at most 33554432 nodes, N <= 321)");
+    if (2 * nflat > kNoAllocPartials) {
+        set_error("hs_dot_noalloc: grid too large for the static scratch (N <= 321, i.e. at most "
+                  "65536 blocks of 512 nodes)");
         return HS_ERR_ARG;
     }
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess || dev < 0 || dev >= 128) {
+    if (e != cudaSuccess) {
         set_error(std::string("hs_dot_noalloc: no current CUDA device: ") + cudaGetErrorString(e));
+        return HS_ERR_CUDA;
+    }
+    if (dev < 0 || dev >= 128) {
+        set_error("hs_dot_noalloc: device ordinal exceeds 128 (the per-device address cache)");
         return HS_ERR_CUDA;
     }
     double* scratch = nullptr;
@@ -70,7 +82,8 @@ extern "C" hs_status hs_dot_noalloc(int N, const double* x, const double* y, dou
         }
         scratch = g_addr[dev];
     }
-    // every partial slot used is written before it is read: nothing to clear
+    // every partial slot read (q = 0, blocks 0..nflat-1) is written by this
+    // call's k_reduce before k_final_dot_noalloc reads it: nothing to clear
     RedArgs r{Nn, nflat, N, RED_DOT, x, y, scratch, nullptr, nullptr};
     k_reduce<<<(int)nflat, RT, 0, 0>>>(r);
     k_final_dot_noalloc<<<1, RT, 0, 0>>>(nflat, out);
