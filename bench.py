@@ -18,8 +18,9 @@ in HBM.  e2e: the same through the public C ABI with host buffers
 working set (~170 MB of node and element arrays) exceeds the 126 MB L2.
 
 --impl reference: the reference path on the host cores: the CPU restatement
-of the reference solver (its dense `fast` element form, colored order), run
-on a bounded sample of the same workload each step.
+of the reference solver (its dense `fast` element form, colored order, all
+host threads); each of its steps is one whole implicit-Euler step of the same
+problem (build_rhs + Jacobi-PCG to rtol 1e-10).
 
 Multi-GPU (torchrun): replicas only -- every rank solves its own seeded
 instance, no collective on the data path; value = all ranks' DOF-iterations
@@ -60,7 +61,6 @@ def parse():
     ap.add_argument("--kernel", default="wht", choices=["wht", "fast", "gauss"])
     ap.add_argument("--scatter", default="colored", choices=["colored", "atomic"])
     ap.add_argument("--no-detect", action="store_true")
-    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-gate", action="store_true",
                     help="skip the supplementary N=256 operator-kernel measurement")
@@ -183,60 +183,90 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_baseline_sample(N, seconds, threads=None, form="fast"):
-    """Time the CPU restatement of the reference solver on a bounded sample of the
-    workload: build_rhs + CG iterations of one implicit-Euler step of the same
-    problem, iterations capped so the sample takes about `seconds`."""
+def host_cpu():
+    """The host's CPU model and logical core count (the CPU baseline's machine)."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"cpu_model": model, "nproc": os.cpu_count()}
+
+
+def reference_problem(N, threads):
+    """The CPU restatement of the reference solver on the bench problem: the
+    reference's dense element form, colored order, ABFT on, same field, IC,
+    dt and tolerance."""
     from oracle import oracle as om
-    n = om.set_threads(threads or os.cpu_count() or 1)
+    n = om.set_threads(threads)
     k, r = make_field(N, 1)
-    o = om.Oracle(N, DT, k, r, form=form, colored=True, detect=True, no_source=True, ic="gaussian",
+    o = om.Oracle(N, DT, k, r, form="fast", colored=True, detect=True, no_source=True, ic="gaussian",
                   ic_sigma=IC_SIGMA)
-    T = o.initial_condition()
-    t0 = time.perf_counter()
-    b = o.build_rhs(T)
-    it1, _, _ = o.pcg(b, T, 1, RTOL)
-    per_iter = max(time.perf_counter() - t0, 1e-3)
-    cap = int(max(1, min(200, seconds / per_iter)))
+    return o, n
+
+
+def reference_step(o, T, cap=500):
+    """One whole implicit-Euler step (build_rhs + Jacobi-PCG to rtol 1e-10):
+    (CG iterations, seconds)."""
     t0 = time.perf_counter()
     b = o.build_rhs(T)
     it, _, _ = o.pcg(b, T, cap, RTOL)
-    dt = time.perf_counter() - t0
+    return it, time.perf_counter() - t0
+
+
+def cpu_baseline_sample(N, one_thread_iters=12):
+    """The reference algorithm on the host cores: one whole implicit-Euler step
+    of the bench problem on all host threads, and a bounded one-thread sample
+    (build_rhs + a few CG iterations of the same step)."""
+    from oracle import oracle as om
+    nproc = os.cpu_count() or 1
+    o, om_threads = reference_problem(N, nproc)
+    T = o.initial_condition()
+    it, dt = reference_step(o, T)
     nodes = (N + 1) ** 3
-    return {"value": nodes * it / dt, "unit": METRIC, "cores": n, "kind": "port",
-            "sample": f"one implicit-Euler step of the same N={N} problem (build_rhs + {it} CG iterations of the "
-                      f"dense reference element form, colored order, ABFT on), {dt:.1f} s on {n} host threads"}
+    om.set_threads(1)
+    it1, dt1 = reference_step(o, T, cap=one_thread_iters)
+    om.set_threads(nproc)
+    return {"value": nodes * it / dt, "unit": METRIC, "cores": om_threads, "kind": "port",
+            "sample": f"one whole implicit-Euler step of the same N={N} problem (build_rhs + {it} CG iterations to "
+                      f"rtol 1e-10, the reference's dense element form, colored order, ABFT on), {dt:.1f} s on "
+                      f"{om_threads} host threads",
+            "value_1thread": nodes * it1 / dt1,
+            "sample_1thread": f"build_rhs + {it1} CG iterations of the same step on 1 thread, {dt1:.1f} s",
+            "host": host_cpu()}
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    from oracle import oracle as om
-    n_threads = om.set_threads(os.cpu_count() or 1)
-    k, r = make_field(args.N, 1)
-    o = om.Oracle(args.N, DT, k, r, form="fast", colored=args.scatter == "colored", detect=not args.no_detect,
-                  no_source=True, ic="gaussian", ic_sigma=IC_SIGMA)
+    o, n_threads = reference_problem(args.N, os.cpu_count() or 1)
     T = o.initial_condition()
-    cap = 3      # CG iterations per bounded sample step
     for _ in range(args.warmup):
-        o.pcg(o.build_rhs(T), T, cap, RTOL)
-    tot_it, t0 = 0, time.perf_counter()
+        reference_step(o, T)
+    tot_it, tot_s = 0, 0.0
     for _ in range(args.steps):
-        it, _, _ = o.pcg(o.build_rhs(T), T, cap, RTOL)
+        it, dt = reference_step(o, T)
         tot_it += it
-    dt = time.perf_counter() - t0
+        tot_s += dt
     nodes = (args.N + 1) ** 3
-    v = nodes * tot_it / dt
+    v = nodes * tot_it / tot_s
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_s / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded lognormal field)",
         "config": dict(workload_config(args, 1), element_form="fast (reference dense 8x8)"),
         "cpu_baseline": {"value": v, "unit": METRIC, "cores": n_threads, "kind": "port",
-                         "sample": f"each step: build_rhs + {cap} CG iterations of one implicit-Euler step of the "
-                                   f"same problem (CPU restatement of the reference solver, dense element form)"},
+                         "sample": f"each step: one whole implicit-Euler step of the same problem (build_rhs + "
+                                   f"Jacobi-PCG to rtol 1e-10, {tot_it / max(1, args.steps):.0f} CG iterations on "
+                                   f"average), the CPU restatement of the reference solver with its dense element "
+                                   f"form, on {n_threads} host threads",
+                         "host": host_cpu()},
         "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -351,7 +381,7 @@ def main():
     if rank == 0 and world == 1 and args.serving_requests > 0:
         line["serving"] = serving_leg(args.serving_requests, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_sample(N, args.cpu_seconds)
+        line["cpu_baseline"] = cpu_baseline_sample(N)
     if rank == 0:
         print(json.dumps(line), flush=True)
     g.close()

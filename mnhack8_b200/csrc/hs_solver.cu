@@ -46,6 +46,21 @@ struct DevBuf {
     ~DevBuf() { if (p) cudaFree(p); }
 };
 
+// CUDA events released on every return path
+struct Events {
+    std::vector<cudaEvent_t> e;
+    cudaError_t create(size_t n) {
+        e.assign(n, nullptr);
+        for (auto& v : e) {
+            const cudaError_t r = cudaEventCreate(&v);
+            if (r != cudaSuccess) { v = nullptr; return r; }
+        }
+        return cudaSuccess;
+    }
+    cudaEvent_t operator[](size_t i) const { return e[i]; }
+    ~Events() { for (auto v : e) if (v) cudaEventDestroy(v); }
+};
+
 inline int grid_for(long long n, int threads, int cap = 148 * 16) {
     long long g = (n + threads - 1) / threads;
     if (g > cap) g = cap;
@@ -743,8 +758,8 @@ hs_status run_case_impl(hs_solver* h, int n_steps, int snap_every, const hs_fi_s
     HS_CUDA(d_it.alloc(std::max(n_steps, 1)));
     HS_CUDA(d_rec.alloc((size_t)std::max(n_steps, 1) * 8));
     HS_CUDA(cudaMemsetAsync(d_rec.p, 0, (size_t)std::max(n_steps, 1) * 8 * 8, h->s));
-    std::vector<cudaEvent_t> ev(2 * (size_t)n_steps);
-    for (auto& e : ev) HS_CUDA(cudaEventCreate(&e));
+    Events ev;
+    HS_CUDA(ev.create(2 * (size_t)n_steps));
     int si = 0;
     for (int step = 0; step < s0; ++step)
         if ((snap_every > 0 && step % snap_every == 0) || step == n_steps - 1) ++si;
@@ -815,7 +830,6 @@ hs_status run_case_impl(hs_solver* h, int n_steps, int snap_every, const hs_fi_s
         o.solve_ms = ms;
         if (keep_reference) { h->ref_tmin[step] = o.tmin; h->ref_tmax[step] = o.tmax; }
     }
-    for (auto& e : ev) cudaEventDestroy(e);
     if (nonfinite) *nonfinite = nf;
     if (T_final_host) HS_CUDA(cudaMemcpy(T_final_host, h->T.p, Nn * 8, cudaMemcpyDeviceToHost));
     return HS_OK;
@@ -845,8 +859,9 @@ hs_status hs_verify(hs_solver* h, int n_steps, double* rel_err, long long* total
     DevBuf<double> d_d1;
     HS_CUDA(d_it.alloc(std::max(n_steps, 1)));
     HS_CUDA(d_d1.alloc(std::max(n_steps, 1)));
-    cudaEvent_t e0, e1;
-    HS_CUDA(cudaEventCreate(&e0)); HS_CUDA(cudaEventCreate(&e1));
+    Events ev2;
+    HS_CUDA(ev2.create(2));
+    cudaEvent_t e0 = ev2[0], e1 = ev2[1];
     HS_CUDA(cudaEventRecord(e0, h->s));
     for (int step = 0; step < n_steps; ++step) {
         st = enqueue_step(h, nullptr, step, 0, d_it.p + step, d_d1.p + step, nullptr, nullptr);
@@ -856,7 +871,6 @@ hs_status hs_verify(hs_solver* h, int n_steps, double* rel_err, long long* total
     HS_CUDA(cudaEventSynchronize(e1));
     float fms = 0.f;
     HS_CUDA(cudaEventElapsedTime(&fms, e0, e1));
-    cudaEventDestroy(e0); cudaEventDestroy(e1);
     std::vector<int> it(std::max(n_steps, 1));
     HS_CUDA(cudaMemcpy(it.data(), d_it.p, n_steps * sizeof(int), cudaMemcpyDeviceToHost));
     long long tot = 0;
@@ -886,8 +900,9 @@ hs_status hs_solve_host(hs_solver* h, const double* T0_host, double* T_host, int
     DevBuf<double> d_d1;
     HS_CUDA(d_it.alloc(std::max(n_steps, 1)));
     HS_CUDA(d_d1.alloc(std::max(n_steps, 1)));
-    cudaEvent_t e0, e1;
-    HS_CUDA(cudaEventCreate(&e0)); HS_CUDA(cudaEventCreate(&e1));
+    Events ev2;
+    HS_CUDA(ev2.create(2));
+    cudaEvent_t e0 = ev2[0], e1 = ev2[1];
     HS_CUDA(cudaEventRecord(e0, h->s));
     HS_CUDA(cudaMemcpyAsync(h->T.p, T0_host, Nn * 8, cudaMemcpyHostToDevice, h->s));
     for (int step = 0; step < n_steps; ++step) {
@@ -899,7 +914,6 @@ hs_status hs_solve_host(hs_solver* h, const double* T0_host, double* T_host, int
     HS_CUDA(cudaEventSynchronize(e1));
     float fms = 0.f;
     HS_CUDA(cudaEventElapsedTime(&fms, e0, e1));
-    cudaEventDestroy(e0); cudaEventDestroy(e1);
     std::vector<int> it(std::max(n_steps, 1));
     HS_CUDA(cudaMemcpy(it.data(), d_it.p, n_steps * sizeof(int), cudaMemcpyDeviceToHost));
     long long tot = 0;
@@ -1009,8 +1023,9 @@ hs_status hs_advance(hs_solver* h, int n_steps, int from_ic, long long* total_it
     DevBuf<double> d_d1;
     HS_CUDA(d_it.alloc(std::max(n_steps, 1)));
     HS_CUDA(d_d1.alloc(std::max(n_steps, 1)));
-    cudaEvent_t e0, e1;
-    HS_CUDA(cudaEventCreate(&e0)); HS_CUDA(cudaEventCreate(&e1));
+    Events ev2;
+    HS_CUDA(ev2.create(2));
+    cudaEvent_t e0 = ev2[0], e1 = ev2[1];
     HS_CUDA(cudaEventRecord(e0, h->s));
     if (from_ic) HS_CUDA(cudaMemcpyAsync(h->T.p, h->T0.p, h->Nn * 8, cudaMemcpyDeviceToDevice, h->s));
     for (int step = 0; step < n_steps; ++step) {
@@ -1021,7 +1036,6 @@ hs_status hs_advance(hs_solver* h, int n_steps, int from_ic, long long* total_it
     HS_CUDA(cudaEventSynchronize(e1));
     float fms = 0.f;
     HS_CUDA(cudaEventElapsedTime(&fms, e0, e1));
-    cudaEventDestroy(e0); cudaEventDestroy(e1);
     std::vector<int> it(std::max(n_steps, 1));
     HS_CUDA(cudaMemcpy(it.data(), d_it.p, n_steps * sizeof(int), cudaMemcpyDeviceToHost));
     long long tot = 0;
@@ -1049,8 +1063,8 @@ hs_status hs_time_kernel(hs_solver* h, int which, int reps, double* ms_per_launc
     const size_t fl = (size_t)32 << 20;   // doubles
     HS_CUDA(flush.alloc(fl));
     HS_CUDA(cudaMemsetAsync(flush.p, 0, fl * 8, h->s));
-    std::vector<cudaEvent_t> ev(2 * (size_t)reps);
-    for (auto& e : ev) HS_CUDA(cudaEventCreate(&e));
+    Events ev;
+    HS_CUDA(ev.create(2 * (size_t)reps));
     const bool det = h->opt.detect != 0;
     // the update finishes the operator's reductions: give it one operator's partials
     if (which == 1) apply_projected(h, ROLE_LOOP, nullptr, h->Ap.p, h->opt.dt, det, h->wA.p, nullptr, 0.0);
@@ -1079,7 +1093,6 @@ hs_status hs_time_kernel(hs_solver* h, int which, int reps, double* ms_per_launc
         HS_CUDA(cudaEventElapsedTime(&ms, ev[2 * r], ev[2 * r + 1]));
         tot += ms;
     }
-    for (auto& e : ev) cudaEventDestroy(e);
     saved.done = 1;
     HS_CUDA(cudaMemcpy(h->st.p, &saved, sizeof(saved), cudaMemcpyHostToDevice));
     if (ms_per_launch) *ms_per_launch = tot / reps;

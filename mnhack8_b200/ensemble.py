@@ -15,6 +15,9 @@ GPU and the same seeded synthetic inputs, and prints one JSON line.
   coverage   detection coverage of the mixed form under 1000 seeded flips
              into its FP32 inner vectors, beside the FP64 drop-in's campaign
              (p, r, Ap) on the same problem (N=64 by default).
+  single     one instance of the batched solver alone (default the N=128
+             bench problem, 2 steps to rtol 1e-8): its device time and
+             inner/outer iteration counts; the short run profiles are taken on.
   serving    a seeded Poisson stream of requests (N uniform in 16..160, steps
              uniform in 10..100, 30 % with one seeded bit flip of the field),
              served by continuous batching: requests join the running batch
@@ -385,6 +388,25 @@ def coverage(N=64, steps=20, flips=1000, seed=21, per_batch=125, rtol=1e-8, inne
             "silent_corruptions": {"mixed": mixed["silent_corruptions"], "fp64": fp64["silent_corruptions"]}}
 
 
+def single(N=128, steps=2, rtol=1e-8, sigma=1.0, corr=8.0, seed=1, device=0):
+    """One instance of the batched mixed-precision solver: lognormal k (sigma,
+    correlation corr elements), Gaussian IC sigma 0.15, dt 1e-4, `steps`
+    implicit-Euler steps to rtol."""
+    k, r = lognormal(N, sigma, corr, seed)
+    b = _lib.Batch(rtol=rtol, device=device)
+    s = b.add(N, 1e-4, k, r, T0=_lib.gaussian_ic(N, 0.15), steps=steps)
+    ms = 0.0
+    while True:
+        n, t = b.step()
+        if not n:
+            break
+        ms += t
+    inf = b.info(s)
+    b.close()
+    return {"N": N, "steps": steps, "ms": ms, "inner_iters": inf["inner_iters"], "outer_iters": inf["outer_iters"],
+            "rel_residual": inf["rel_residual"]}
+
+
 def _main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -400,6 +422,9 @@ def _main(argv=None):
     p.add_argument("--flips", type=int, default=1000)
     p.add_argument("--rows", default=None, help="write the mixed form's per-flip rows (JSON) here")
     p.add_argument("--no-fp64", action="store_true")
+    p = sub.add_parser("single")
+    p.add_argument("--N", type=int, default=128)
+    p.add_argument("--steps", type=int, default=2)
     p = sub.add_parser("serving")
     p.add_argument("--n", type=int, default=400)
     p.add_argument("--rate", type=float, default=200.0)
@@ -411,6 +436,8 @@ def _main(argv=None):
         out = coverage(N=a.N, flips=a.flips, rows_out=a.rows, fp64=not a.no_fp64)
     elif a.cmd == "batching":
         out = batching(n=a.n, steps=a.steps, serial_sample=a.serial_sample)
+    elif a.cmd == "single":
+        out = single(N=a.N, steps=a.steps)
     else:
         out = serving(n=a.n, rate=a.rate, max_live=a.max_live)
     print(json.dumps(out), flush=True)

@@ -7,7 +7,7 @@ mounted) the recorded outputs of the reference validation suite
 ``tests/golden/reference_v10.json``.  The JSON is the fixture the tests use;
 nothing at test time reads the reference tree.
 
-Usage:  python tests/golden/make_golden.py [REFERENCE_ROOT]
+Usage:  python tests/golden/make_golden.py REFERENCE_ROOT
 """
 from __future__ import annotations
 
@@ -21,7 +21,9 @@ import tempfile
 
 import numpy as np
 
-ROOT = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: python tests/golden/make_golden.py REFERENCE_ROOT")
+ROOT = sys.argv[1]
 V10 = os.path.join(ROOT, "tests", "baseline_validation", "v10")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_v10.json")
 
