@@ -93,9 +93,10 @@ typedef struct hs_step_record {
     double solve_ms;    /* build_rhs + PCG (+ reprojection) device time of the step */
 } hs_step_record;
 
-/* canonical reduction orders of an N-element grid: the operator's slab tile
- * (planes cx, rows ty, columns tz; rt threads of bpt positions each, halo
- * included) and the flat order's nodes per thread kf */
+/* canonical reduction orders of an N-element grid: the operator's column
+ * partition (cx planes per x-slab, ty node rows per lane, tz node columns per
+ * full warp segment, rt threads = bpt warps per tile) and the flat order's
+ * nodes per thread kf */
 typedef struct hs_layout_info { int cx, ty, tz, rt, bpt, kf; } hs_layout_info;
 
 void        hs_default_options(hs_options* opt);
