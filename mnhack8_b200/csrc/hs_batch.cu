@@ -145,8 +145,9 @@ hs_status upload(hs_batch* b) {
         b->cap_flat = std::max<long long>({nf, 2 * b->cap_flat, 1024});
         HS_CUDA(b->d_t2i.alloc(b->cap_tiles));
         HS_CUDA(b->d_f2i.alloc(b->cap_flat));
-        HS_CUDA(b->pa.alloc((size_t)MAXQ * b->cap_tiles));
-        HS_CUDA(b->pf.alloc((size_t)4 * b->cap_flat));
+        // compensated partials: (hi, lo) per quantity
+        HS_CUDA(b->pa.alloc((size_t)2 * MAXQ * b->cap_tiles));
+        HS_CUDA(b->pf.alloc((size_t)2 * 4 * b->cap_flat));
         if (b->gexec) { cudaGraphExecDestroy(b->gexec); b->gexec = nullptr; }
         if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
     }

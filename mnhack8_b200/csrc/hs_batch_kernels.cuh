@@ -7,10 +7,56 @@
 // an FP32 Jacobi-PCG solve of A d = r to a loose relative tolerance (FP32
 // operator and preconditioner, FP64 dot products of the FP32 values), and
 // T += d in FP64, until ||b - A T|| / ||b|| < rtol.
+// The CG dot products, the outer residual and the ABFT checksum sums are
+// accumulated in FP64 with compensation (hs_csum.h): every partial is a pair
+// (hi, lo), stored as quantity q and q + NQ, and merged pair-wise.
 #pragma once
 #include "hs_kernels.cuh"
+#include "hs_csum.h"
 
 namespace hs {
+
+// canonical block tree (as cta_tree_sum) over compensated pairs; sh holds
+// 2*NQ rows of 8; result valid in thread 0
+template <int NQ>
+__device__ __forceinline__ void cta_tree_csum(CSum (&v)[NQ], double (*sh)[8]) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+#pragma unroll
+        for (int off = 16; off >= 1; off >>= 1) {
+            const CSum o{__shfl_xor_sync(0xffffffffu, v[q].hi, off), __shfl_xor_sync(0xffffffffu, v[q].lo, off)};
+            csum_merge(v[q], o);
+        }
+    }
+    __syncthreads();
+    if (lane == 0 && warp < 8) {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) { sh[q][warp] = v[q].hi; sh[NQ + q][warp] = v[q].lo; }
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            CSum u{(lane < 8) ? sh[q][lane] : 0.0, (lane < 8) ? sh[NQ + q][lane] : 0.0};
+#pragma unroll
+            for (int off = 4; off >= 1; off >>= 1) {
+                const CSum o{__shfl_xor_sync(0xffffffffu, u.hi, off), __shfl_xor_sync(0xffffffffu, u.lo, off)};
+                csum_merge(u, o);
+            }
+            v[q] = u;
+        }
+    }
+}
+// store a block's compensated partials: hi as quantity q, lo as q + NQ
+template <int NQ>
+__device__ __forceinline__ void store_cpartials(const CSum (&v)[NQ], double* base, long long stride, long long idx) {
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+        base[q * stride + idx] = v[q].hi;
+        base[(NQ + q) * stride + idx] = v[q].lo;
+    }
+}
 
 // per-instance scalars, device resident
 struct BState {
@@ -128,7 +174,7 @@ template <typename V>
 struct __align__(16) BSlabSmem {
     V P[2][SPOS];
     typename VTraits<V>::V2 Y1[SPOS], Y2[SPOS], Y3[SPOS];
-    double sh[MAXQ][8];
+    double sh[2 * MAXQ][8];
 };
 
 // Batched slab operator.  KIND 0: y64 = A T (FP64, residual); 1: b = M T
@@ -183,7 +229,7 @@ __device__ __forceinline__ void kb_tile(const BatchArgs& B, BSlabSmem<V>& S, lon
     const bool two = src_b != nullptr;
     const double* w = (KIND == BK_RHS) ? I.wM : I.wA;
     const bool d1 = B.detect != 0;
-    double part[MAXQ] = {0.0, 0.0, 0.0, 0.0};
+    CSum part[MAXQ] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
 
     V pA[SK], pB[SK], aA[SK], aB[SK], ra[SK], rb[SK], cr[SK], ckk[SK];
     double wv[SK];
@@ -289,11 +335,11 @@ __device__ __forceinline__ void kb_tile(const BatchArgs& B, BSlabSmem<V>& S, lon
                     if (fi_ap && (long long)n == fi_idx) { y = flipf(y, fi_bit); st->fi_fired = 1; }
                 }
                 const double pv = (double)pc[k], yd = (double)y;
-                if (loop) part[0] = dfma(pv, yd, part[0]);
+                if (loop) csum_fma(part[0], pv, yd);
                 if (d1) {
-                    part[1] = bnd ? part[1] : dadd(part[1], yd);
-                    part[2] = dfma(wv[k], pv, part[2]);
-                    part[3] = dfma(pv, pv, part[3]);
+                    if (!bnd) csum_add(part[1], yd);
+                    csum_fma(part[2], wv[k], pv);
+                    part[3].hi = dfma(pv, pv, part[3].hi);      // the norm only scales the threshold
                 }
                 __stwb(yout + n, y);                      // global stores (the pointers come from global memory)
                 if (loop) __stwb(pout + n, pc[k]);
@@ -314,11 +360,8 @@ __device__ __forceinline__ void kb_tile(const BatchArgs& B, BSlabSmem<V>& S, lon
         for (int k = 0; k < SK; ++k) { pA[k] = pB[k]; aA[k] = aB[k]; }
     }
     if (!loop && !d1) return;
-    cta_tree_sum<MAXQ>(part, S.sh);
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int q = 0; q < MAXQ; ++q) B.pa[q * B.ntiles + t] = part[q];
-    }
+    cta_tree_csum<MAXQ>(part, S.sh);
+    if (threadIdx.x == 0) store_cpartials<MAXQ>(part, B.pa, B.ntiles, t);
 }
 
 template <typename V, int KIND>
@@ -339,29 +382,35 @@ __global__ void __launch_bounds__(ST, 2) kb_apply(BatchArgs B) {
     }
 }
 
-// sums of one instance's partials (count values at stride qstride per quantity)
+// compensated sums of one instance's partials: count (hi, lo) pairs per
+// quantity, hi of quantity q at base + q*qstride, lo at base + (q+NQ)*qstride;
+// RT strided sequential merges, then the block tree; valid in thread 0
 template <int NQ>
 __device__ __forceinline__ void inst_sums(double (&v)[NQ], const double* base, long long count, long long qstride,
                                           double (*sh)[8]) {
-    constexpr int FB = 16;
+    constexpr int FB = 8;
+    CSum acc[NQ];
 #pragma unroll
-    for (int q = 0; q < NQ; ++q) v[q] = 0.0;
+    for (int q = 0; q < NQ; ++q) acc[q] = CSum{0.0, 0.0};
     for (long long k0 = threadIdx.x; k0 < count; k0 += (long long)RT * FB) {
-        double t[NQ][FB];
+        double th[NQ][FB], tl[NQ][FB];
 #pragma unroll
         for (int q = 0; q < NQ; ++q)
 #pragma unroll
             for (int u = 0; u < FB; ++u) {
                 const long long k = k0 + (long long)u * RT;
-                t[q][u] = (k < count) ? __ldcg(base + q * qstride + k) : 0.0;
+                th[q][u] = (k < count) ? __ldcg(base + q * qstride + k) : 0.0;
+                tl[q][u] = (k < count) ? __ldcg(base + (NQ + q) * qstride + k) : 0.0;
             }
 #pragma unroll
         for (int q = 0; q < NQ; ++q)
 #pragma unroll
             for (int u = 0; u < FB; ++u)
-                if (k0 + (long long)u * RT < count) v[q] = dadd(v[q], t[q][u]);
+                if (k0 + (long long)u * RT < count) csum_merge(acc[q], CSum{th[q][u], tl[q][u]});
     }
-    cta_tree_sum<NQ>(v, sh);
+    cta_tree_csum<NQ>(acc, sh);
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) v[q] = csum_value(acc[q]);
 }
 
 __device__ __forceinline__ double d1_rel(const double (&p)[MAXQ], double nw) {
@@ -374,7 +423,7 @@ __device__ __forceinline__ double d1_rel(const double (&p)[MAXQ], double nw) {
 // one block per instance: operator partials -> D1 (and alpha in the loop)
 template <int KIND>
 __global__ void __launch_bounds__(RT) kb_final_apply(BatchArgs B) {
-    __shared__ double sh[MAXQ][8];
+    __shared__ double sh[2 * MAXQ][8];
     const int slot = blockIdx.x;
     if (slot >= B.n_inst) return;
     const BInst& I = B.inst[slot];
@@ -421,9 +470,9 @@ __device__ __forceinline__ FlatPos flat_pos(const BatchArgs& B) {
 // residual r = b - A T in FP64 and the start of an inner solve:
 // r32 = r, z32 = r32 / d, d32 = 0; partials r.r, b.b (FP64), r32.z32, r32.r32
 __global__ void __launch_bounds__(RT) kb_resid(BatchArgs B) {
-    __shared__ double sh[MAXQ][8];
+    __shared__ double sh[2 * MAXQ][8];
     const FlatPos f = flat_pos(B);
-    double part[4] = {0.0, 0.0, 0.0, 0.0};
+    CSum part[4] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
     if (f.slot >= 0) {
         const BInst& I = B.inst[f.slot];
         if (I.active && !I.st->odone) {
@@ -435,23 +484,20 @@ __global__ void __launch_bounds__(RT) kb_resid(BatchArgs B) {
                 const float r32 = (float)rv;
                 const float z = __fmul_rn(r32, I.dinv32[m]);
                 I.r32[m] = r32; I.z32[m] = z; I.d32[m] = 0.f;
-                part[0] = dfma(rv, rv, part[0]);
-                part[1] = dfma(bv, bv, part[1]);
-                part[2] = dfma((double)r32, (double)z, part[2]);
-                part[3] = dfma((double)r32, (double)r32, part[3]);
+                csum_fma(part[0], rv, rv);
+                csum_fma(part[1], bv, bv);
+                csum_add(part[2], dmul((double)r32, (double)z));     // products of FP32 values are exact
+                csum_add(part[3], dmul((double)r32, (double)r32));
             }
         }
     }
-    cta_tree_sum<4>(part, sh);
-    if (threadIdx.x == 0 && blockIdx.x < B.nflat) {
-#pragma unroll
-        for (int q = 0; q < 4; ++q) B.pf[q * B.nflat + blockIdx.x] = part[q];
-    }
+    cta_tree_csum<4>(part, sh);
+    if (threadIdx.x == 0 && blockIdx.x < B.nflat) store_cpartials<4>(part, B.pf, B.nflat, blockIdx.x);
 }
 
 // one block per instance: outer convergence test and the inner solve's start
 __global__ void __launch_bounds__(RT) kb_outer_final(BatchArgs B) {
-    __shared__ double sh[MAXQ][8];
+    __shared__ double sh[2 * MAXQ][8];
     const int slot = blockIdx.x;
     if (slot >= B.n_inst) return;
     const BInst& I = B.inst[slot];
@@ -486,9 +532,9 @@ __global__ void __launch_bounds__(RT) kb_outer_final(BatchArgs B) {
 
 // inner FP32 update: d += alpha p, r -= alpha Ap, z = r / diag; partials r.r, r.z
 __global__ void __launch_bounds__(RT) kb_update32(BatchArgs B) {
-    __shared__ double sh[MAXQ][8];
+    __shared__ double sh[2 * MAXQ][8];
     const FlatPos f = flat_pos(B);
-    double part[2] = {0.0, 0.0};
+    CSum part[2] = {{0.0, 0.0}, {0.0, 0.0}};
     if (f.slot >= 0) {
         const BInst& I = B.inst[f.slot];
         const BState* st = I.st;
@@ -524,8 +570,8 @@ __global__ void __launch_bounds__(RT) kb_update32(BatchArgs B) {
                 rv[k] = r;
                 zv[k] = __fmul_rn(r, iv[k]);
                 if (k < f.cnt) {
-                    part[0] = dfma((double)r, (double)r, part[0]);
-                    part[1] = dfma((double)r, (double)zv[k], part[1]);
+                    csum_add(part[0], dmul((double)r, (double)r));         // exact products
+                    csum_add(part[1], dmul((double)r, (double)zv[k]));
                 }
             }
             if (f.cnt == 2) {
@@ -537,13 +583,13 @@ __global__ void __launch_bounds__(RT) kb_update32(BatchArgs B) {
             }
         }
     }
-    cta_tree_sum<2>(part, sh);
-    if (threadIdx.x == 0 && blockIdx.x < B.nflat) { B.pf[blockIdx.x] = part[0]; B.pf[B.nflat + blockIdx.x] = part[1]; }
+    cta_tree_csum<2>(part, sh);
+    if (threadIdx.x == 0 && blockIdx.x < B.nflat) store_cpartials<2>(part, B.pf, B.nflat, blockIdx.x);
 }
 
 // one block per instance: inner convergence and beta
 __global__ void __launch_bounds__(RT) kb_final_update32(BatchArgs B) {
-    __shared__ double sh[MAXQ][8];
+    __shared__ double sh[2 * MAXQ][8];
     const int slot = blockIdx.x;
     if (slot >= B.n_inst) return;
     const BInst& I = B.inst[slot];
