@@ -68,6 +68,9 @@ def parse():
                     help="requests of the supplementary serving measurement (0: skip)")
     ap.add_argument("--profile", action="store_true",
                     help="only the timed trajectories (no e2e, kernel timing or CPU baseline): for ncu captures")
+    ap.add_argument("--profile-kernel", action="store_true",
+                    help="only a few launches of the PCG operator kernel at --N (L2 scrubbed before each): "
+                         "for one-launch ncu captures")
     return ap.parse_args()
 
 
@@ -280,6 +283,8 @@ def main():
     import torch
     from mnhack8_b200 import _lib
 
+    if args.profile_kernel:
+        return profile_kernel(args)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -392,6 +397,22 @@ def main():
 
 
 GATE_N = 256
+
+
+def profile_kernel(args):
+    """Three launches of the PCG operator kernel on the bench's field at --N
+    (the L2 scrubbed before each), timed with CUDA events; prints one JSON line."""
+    from mnhack8_b200 import _lib
+    N = args.N
+    k, r = make_field(N, 1)
+    g = _lib.Solver(N, DT, k, r, kernel=args.kernel, scatter=args.scatter, detect=not args.no_detect,
+                    no_source=True, ic="gaussian", ic_sigma=IC_SIGMA, rtol=RTOL, max_iter=500, device=0)
+    ms = g.time_kernel(0, reps=3)
+    g.close()
+    alg = (40 if not args.no_detect else 32) * (N + 1) ** 3 + 16 * N ** 3
+    print(json.dumps({"N": N, "ms_per_launch": ms, "alg_bytes_per_launch": alg,
+                      "achieved_gbs": alg / (ms * 1e-3) / 1e9}), flush=True)
+    return 0
 
 
 def serving_leg(n, device):

@@ -142,3 +142,23 @@ def test_v6_coverage_cases(ln32_runs, golden, oracle, case):
     assert s["iters_delta_max"] == int(sm["iters_delta_max"])
     if sm["class"] != "detected":
         assert "%.6e" % s["E_fault_max"] == sm["E_fault_max"]
+
+
+def test_v3_boundary_control(oracle, golden):
+    """V3 boundary control: a level-G bit-62 flip of a boundary node (0, N/2,
+    N/2) at step 10 leaves a BC-scheme artifact that --reproject-bc removes.
+    E_max / E_final and the class match the recorded run to their printed
+    digits, with and without reprojection."""
+    g = golden["v3"]["boundary_control"]
+    N = 32
+    k, r = field(N, "lognormal", sigma=1.0, L=0.125, seed=7)
+    o = oracle.Oracle(N, 5e-4, k, r, form="fast", colored=True)
+    rA = o.run_case(40, snap_every=1, keep_snaps=True)
+    rB = o.run_case(40, snap_every=1, ref_snaps=rA["snaps"])
+    bnode = (N // 2) * (N + 1) + N // 2
+    for key, rep in (("no_reproject", False), ("reproject", True)):
+        rF = o.run_case(40, snap_every=1, fi=(1, 10, bnode, 62, 0), ref_snaps=rA["snaps"], reproject=rep)
+        s = oracle.classify(rA, rB, rF, 1, 5e-4)
+        assert s["cls"] == g[key]["class"]
+        assert "%.6e" % s["E_fault_max"] == "%.6e" % g[key]["E_max"]
+        assert "%.6e" % s["E_fault_final"] == "%.6e" % g[key]["E_final"]
