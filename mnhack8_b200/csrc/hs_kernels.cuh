@@ -349,22 +349,68 @@ struct UpdateArgs {
     long long nblk;             // LOOP: their count per quantity
 };
 
+// PCG scalar logic after the vector update, on the FLAT-order sums: the
+// prologue's ||b||, rho and initial residual, or the loop's convergence test
+// (||r||/||b|| < tol, the reference's recursive residual), beta = rho_new /
+// rho and the iteration count; sets the graph's while condition.
+__device__ __forceinline__ void update_scalars(const UpdateArgs& a, const double (&part)[3]) {
+    DevState* st = a.st;
+    if (a.role == UPD_PRE) {
+        double bnorm = __dsqrt_rn(part[0]);
+        if (bnorm < 1e-30) bnorm = 1.0;
+        st->bnorm = bnorm;
+        st->rho = part[1];
+        st->rel0 = __ddiv_rn(__dsqrt_rn(part[2]), bnorm);
+        st->iter = 0; st->broken = 0; st->result = 0; st->beta = 0.0;
+        st->done = (st->max_iter <= 0) ? 1 : 0;
+    } else {
+        const int iter = st->iter;
+        const double rnorm = __dsqrt_rn(part[0]);
+        const double rel = __ddiv_rn(rnorm, st->bnorm);
+        const bool conv = rel < st->tol;
+        double beta = 0.0;
+        if (!conv) { beta = __ddiv_rn(part[1], st->rho); st->rho = part[1]; }
+        if (st->log_rel && iter < st->log_cap) {
+            st->log_rel[iter] = rel; st->log_alpha[iter] = st->alpha; st->log_beta[iter] = beta;
+        }
+        st->beta = beta;
+        if (conv) { st->result = iter + 1; st->done = 1; }
+        else {
+            st->iter = iter + 1;
+            if (iter + 1 >= st->max_iter) { st->done = 1; st->result = st->max_iter; }
+        }
+        if (a.use_cond) cudaGraphSetConditional(a.cond, st->done ? 0u : 1u);
+    }
+}
+
 // PCG vector update on the flat partition: each thread updates its KF
 // consecutive nodes (KF / 2 aligned 128-bit loads and stores per vector), in
-// order.  In the loop it also finishes the operator's reductions: every CTA
+// order.  In the loop it first finishes the operator's reductions: every CTA
 // sums p.Ap over the tile partials in the canonical order (so alpha = rho /
 // p.Ap is the same bits everywhere), and CTA 0 records p.Ap, alpha, the D1
-// checksum and a breakdown, the work a separate single-CTA kernel would do.
-constexpr int kUpdateCtasPerSm = 5;
-__global__ void __launch_bounds__(RT, kUpdateCtasPerSm) k_update(UpdateArgs a) {
+// checksum and a breakdown.
+//
+// It also finishes its own reductions.  The FLAT order's final pass gives
+// thread l of its block tree the partials of blocks l, l+RT, l+2RT, ... added
+// in that order; the kernel runs exactly RT CTAs and CTA c visits the blocks
+// c, c+RT, ... in increasing order (two at a time), so CTA c forms thread c's
+// sequential sum itself.  The last CTA to finish (an atomic ticket) combines
+// the RT sums with the block tree and runs the scalar logic.
+constexpr int kUpdateCtas = RT;
+__global__ void __launch_bounds__(RT, 2) k_update(UpdateArgs a) {
     static_assert(KF % 2 == 0, "pairs of nodes per thread");
     constexpr int NC = KF / 2;
-    __shared__ double sh[MAXQ][8];
+    __shared__ double sh[6][8];
     __shared__ double s_pAp;
+    __shared__ unsigned s_last;
     DevState* st = a.st;
     const int tid = threadIdx.x;
-    if (a.role == UPD_LOOP && st->done) return;
     const bool pre = a.role == UPD_PRE;
+    if (!pre && st->done) {
+        // the solve ended (converged, capped or broken down): end the graph's while loop
+        if (a.use_cond && blockIdx.x == 0 && tid == 0) cudaGraphSetConditional(a.cond, 0u);
+        return;
+    }
     int iter = 0;
     double alpha = 0.0;
     const double* p = nullptr;
@@ -387,8 +433,12 @@ __global__ void __launch_bounds__(RT, kUpdateCtasPerSm) k_update(UpdateArgs a) {
                     st->d1_step = fmax(st->d1_step, rel);
                 }
                 st->pAp = q[0];
-                if (fabs(q[0]) < 1e-30) { st->broken = 1; st->done = 1; st->result = st->iter; }
-                else st->alpha = __ddiv_rn(st->rho, q[0]);
+                if (fabs(q[0]) < 1e-30) {
+                    st->broken = 1; st->done = 1; st->result = st->iter;
+                    if (a.use_cond) cudaGraphSetConditional(a.cond, 0u);
+                } else {
+                    st->alpha = __ddiv_rn(st->rho, q[0]);
+                }
                 s_pAp = q[0];
             }
         } else {
@@ -402,15 +452,14 @@ __global__ void __launch_bounds__(RT, kUpdateCtasPerSm) k_update(UpdateArgs a) {
         alpha = __ddiv_rn(st->rho, pAp);
     }
     const double nalpha = -alpha;
-    // flat blocks blockIdx.x, + gridDim.x, ...; each block's partials at its own index
-    for (long long blk = blockIdx.x; blk < a.nflat; blk += gridDim.x) {
-        double part[3] = {0.0, 0.0, 0.0};   // PRE: bb, rz, rr   LOOP: rr, rz, -
+    // one flat block: its 3 partials (PRE: bb, rz, rr   LOOP: rr, rz, -) into part
+    auto block = [&](long long blk, double* part) {
         const long long m0 = (blk * RT + tid) * KF;
         int cnt[NC];
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
             const long long m = m0 + 2 * c;
-            cnt[c] = (m + 1 < a.Nn) ? 2 : (m < a.Nn ? 1 : 0);
+            cnt[c] = (blk >= a.nflat) ? 0 : (m + 1 < a.Nn) ? 2 : (m < a.Nn ? 1 : 0);
         }
         auto ld = [&](const double* base, double (&v)[KF]) {
 #pragma unroll
@@ -459,61 +508,42 @@ __global__ void __launch_bounds__(RT, kUpdateCtasPerSm) k_update(UpdateArgs a) {
             }
             stv(a.x, xx); stv(a.r, rr); stv(a.z, dd);
         }
-        cta_tree_sum<3>(part, sh);
+    };
+    // this CTA's strided sequential sums (thread blockIdx.x of the final pass), in thread 0
+    double seq[3] = {0.0, 0.0, 0.0};
+    const long long G = gridDim.x;
+    for (long long b0 = blockIdx.x; b0 < a.nflat; b0 += 2 * G) {
+        double part[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        block(b0, part);
+        block(b0 + G, part + 3);
+        cta_tree_sum<6>(part, sh);
         if (tid == 0) {
 #pragma unroll
-            for (int q = 0; q < 3; ++q) a.partials[q * a.nflat + blk] = part[q];
+            for (int q = 0; q < 3; ++q) seq[q] = dadd(seq[q], part[q]);
+            if (b0 + G < a.nflat) {
+#pragma unroll
+                for (int q = 0; q < 3; ++q) seq[q] = dadd(seq[q], part[3 + q]);
+            }
         }
     }
-}
-
-// PCG scalar logic after the vector update: the prologue's ||b||, rho and
-// initial residual, or the loop's convergence test (||r||/||b|| < tol, the
-// reference's recursive residual), beta = rho_new / rho and the iteration
-// count; sets the graph's while condition.
-struct FinalUpdateArgs {
-    const double* partials;
-    long long nflat;
-    DevState* st;
-    cudaGraphConditionalHandle cond;
-    int role, use_cond;
-};
-__global__ void __launch_bounds__(RT) k_final_update(FinalUpdateArgs a) {
-    __shared__ double sh[MAXQ][8];
-    DevState* st = a.st;
-    const bool pre = a.role == UPD_PRE;
-    if (!pre && st->done) {
-        if (a.use_cond && threadIdx.x == 0) cudaGraphSetConditional(a.cond, 0u);
-        return;
+    if (tid == 0) {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) a.partials[q * RT + blockIdx.x] = seq[q];
+        __threadfence();
+        const unsigned t = atomicAdd(a.ticket, 1u);
+        s_last = (t == gridDim.x - 1) ? 1u : 0u;
     }
-    double part[3];
-    final_sums<3>(part, a.partials, a.nflat, sh);
-    if (threadIdx.x != 0) return;
-    if (pre) {
-        double bnorm = __dsqrt_rn(part[0]);
-        if (bnorm < 1e-30) bnorm = 1.0;
-        st->bnorm = bnorm;
-        st->rho = part[1];
-        st->rel0 = __ddiv_rn(__dsqrt_rn(part[2]), bnorm);
-        st->iter = 0; st->broken = 0; st->result = 0; st->beta = 0.0;
-        st->done = (st->max_iter <= 0) ? 1 : 0;
-    } else {
-        const int iter = st->iter;
-        const double rnorm = __dsqrt_rn(part[0]);
-        const double rel = __ddiv_rn(rnorm, st->bnorm);
-        const bool conv = rel < st->tol;
-        double beta = 0.0;
-        if (!conv) { beta = __ddiv_rn(part[1], st->rho); st->rho = part[1]; }
-        if (st->log_rel && iter < st->log_cap) {
-            st->log_rel[iter] = rel; st->log_alpha[iter] = st->alpha; st->log_beta[iter] = beta;
-        }
-        st->beta = beta;
-        if (conv) { st->result = iter + 1; st->done = 1; }
-        else {
-            st->iter = iter + 1;
-            if (iter + 1 >= st->max_iter) { st->done = 1; st->result = st->max_iter; }
-        }
-        if (a.use_cond) cudaGraphSetConditional(a.cond, st->done ? 0u : 1u);
+    __syncthreads();
+    if (!s_last) return;
+    // the last CTA: block tree over the RT sums, then the scalar logic
+    __threadfence();
+    double v[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) v[q] = __ldcg(a.partials + q * RT + tid);
+    cta_tree_sum<3>(v, sh);
+    if (tid == 0) {
+        *a.ticket = 0u;
+        update_scalars(a, v);
     }
 }
 
