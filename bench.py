@@ -64,8 +64,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-gate", action="store_true",
                     help="skip the supplementary N=256 operator-kernel measurement")
-    ap.add_argument("--serving-requests", type=int, default=48,
+    ap.add_argument("--serving-requests", type=int, default=300,
                     help="requests of the supplementary serving measurement (0: skip)")
+    ap.add_argument("--batching-instances", type=int, default=256,
+                    help="instances of the supplementary batching measurement (0: skip)")
     ap.add_argument("--profile", action="store_true",
                     help="only the timed trajectories (no e2e, kernel timing or CPU baseline): for ncu captures")
     ap.add_argument("--profile-kernel", action="store_true",
@@ -383,6 +385,8 @@ def main():
     }
     if rank == 0 and not args.no_gate and N != GATE_N:
         line["apply_gate_N256"] = gate_apply(local, detect, args.kernel, args.scatter)
+    if rank == 0 and world == 1 and args.batching_instances > 0:
+        line["batching"] = batching_leg(args.batching_instances, local)
     if rank == 0 and world == 1 and args.serving_requests > 0:
         line["serving"] = serving_leg(args.serving_requests, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -419,11 +423,29 @@ def serving_leg(n, device):
     """Supplementary: served solves/s and p50 / p99 latency of the batched
     mixed-precision server beside serial plain FP64 on this GPU, for the first
     n requests of the seeded serving stream (Poisson 200/s, N 16..160, 10..100
-    steps, 30 % flipped, rtol 1e-8); fields are generated before timing."""
+    steps, 30 % flipped, rtol 1e-8); fields are generated before timing (their
+    per-request generation time is reported beside the latencies)."""
     from mnhack8_b200 import ensemble
     r = ensemble.serving(n=n, device=device)
     return {"requests": n, "stream": "Poisson 200/s, N 16..160, steps 10..100, 30% one bit flip, rtol 1e-8",
-            "batched": r["batched"], "serial_fp64": r["serial_fp64"], "solves_per_s_ratio": r["throughput_ratio"]}
+            "stream_span_s": r["stream_span_s"], "peak_live": r["peak_live"],
+            "batched": r["batched"], "serial_fp64": r["serial_fp64"], "solves_per_s_ratio": r["throughput_ratio"],
+            "field_generation": r["field_generation"]}
+
+
+def batching_leg(n, device):
+    """Supplementary: the ensemble of n independent solves (N uniform in
+    16..96, lognormal k sigma 1 with correlation N/8 elements, 20 steps to
+    rtol 1e-8) in one batch (one graph launch per step, autotuned tile depth)
+    beside the same solves one at a time through the plain FP64 drop-in."""
+    from mnhack8_b200 import ensemble
+    r = ensemble.batching(n=n, device=device)
+    keep = ("instances", "N_range", "steps", "rtol", "tile_planes", "autotune_ms_per_tile_planes", "batch_ms",
+            "batch_solves_per_s", "serial_fp64_ms", "serial_fp64_solves_per_s", "serial_fp64_timed_solves",
+            "max_final_true_rel_residual")
+    out = {k: r[k] for k in keep}
+    out["solves_per_s_ratio"] = r["speedup_vs_serial_fp64"]
+    return out
 
 
 def gate_apply(device, detect, kernel, scatter):
