@@ -9,6 +9,7 @@
 // planes of its x-slab, so the element rows and planes above and below are in
 // its own registers.
 //
+// A slab's march starts one layer early, forming its lower halo plane xa-1.
 // Step i of layer x (elements between planes x and x+1):
 //   1. forms p at node row r = r0-1+i of plane x+1, columns c and c+1 (the
 //      PCG loop's p = z + beta p_{k-1}, or the input vector), stores p and
@@ -115,7 +116,7 @@ __device__ __forceinline__ void col_march(const ApplyArgs& a, const ColLane& C, 
             B.b1 = v1 ? __ldg(srcB + n + 1) : 0.0;
         }
         B.w = (d1 && v0 && xp >= xa && xp <= xb && ((orow >> i) & 1u)) ? __ldg(a.w + n) : 0.0;
-        const bool ev = i >= 1 && x >= 0 && x < N && ecv && ((erowv >> i) & 1u);
+        const bool ev = i >= 1 && x >= xa - 1 && x >= 0 && x < N && ecv && ((erowv >> i) & 1u);
         const double2 c = ev ? __ldg(a.coef + (x * N * N + lane_e + i * N)) : make_double2(0.0, 0.0);
         B.cr = c.x;
         B.ck = c.y;
@@ -134,13 +135,15 @@ __device__ __forceinline__ void col_march(const ApplyArgs& a, const ColLane& C, 
     for (int i = 0; i < NS; ++i) pl[i][0] = pl[i][1] = 0.0;
     ColStep B0, B1, B2;
     B0.b0 = B0.b1 = B1.b0 = B1.b1 = B2.b0 = B2.b1 = 0.0;
-    load(B0, xa - 1, 0);
-    load(B1, xa - 1, 1);
+    load(B0, xa - 2, 0);
+    load(B1, xa - 2, 1);
 
-    for (int x = xa - 1; x <= xb; ++x) {
-        const bool el = x >= 0 && x < N;       // element layer x exists
-        const bool cpl = x >= xa;              // plane x is the task's: complete its nodes
-        const bool fown = x + 1 <= xb;         // plane x+1 is the task's: store p, w.p, p.p
+    // layer xa-2 only forms plane xa-1 (the slab's lower halo plane); layers
+    // xa-1 .. xb apply their elements
+    for (int x = xa - 2; x <= xb; ++x) {
+        const bool el = x >= xa - 1 && x >= 0 && x < N;   // element layer x is applied
+        const bool cpl = x >= xa;                          // plane x is the task's: complete its nodes
+        const bool fown = x + 1 >= xa && x + 1 <= xb;      // plane x+1 is the task's: store p, w.p, p.p
         double zsP_s = 0.0, zsP_d = 0.0;       // z butterfly of the previous row
         double pnA = 0.0, pnB = 0.0;           // p of the previous row (plane x+1)
         double hq2 = 0.0, hL3 = 0.0, hq6 = 0.0, hL7 = 0.0;   // element row below: its oy = 1 outputs
