@@ -270,6 +270,16 @@ void      hs_batch_destroy(hs_batch* b);
  * instance takes n_steps steps.  Sets *slot. */
 hs_status hs_batch_add(hs_batch* b, int N, double dt, const double* k, const double* rhoc, const double* T0,
                        int n_steps, int* slot);
+/* As hs_batch_add, with the instance's conductivity generated on the device:
+ * a periodic Gaussian field of covariance exp(-r^2/L^2) (L in domain units),
+ * standardised, k = exp(mu + sigma g), rho*c = rhoc.  The reference draws
+ * these fields on the host with scripts/gen_field.py:29-61 (NumPy's random
+ * stream and FFT); this generator has the same law but its own counter-based
+ * random stream (see hs_field_lognormal), so the field is a fixed function of
+ * (N, seed, L, mu, sigma) and is not the reference file bit for bit.
+ * No host field crosses the bus; the generation runs on the add stream. */
+hs_status hs_batch_add_lognormal(hs_batch* b, int N, double dt, double mu, double sigma, double L,
+                                 unsigned long long seed, double rhoc, const double* T0, int n_steps, int* slot);
 /* level-G fault: flip bit `bit` of T[idx % (N+1)^3] before the instance's step `step` */
 hs_status hs_batch_arm_flip(hs_batch* b, int slot, int step, long long idx, int bit);
 /* fault in an FP32 inner vector: level HS_FI_P (p after formation), HS_FI_RV
@@ -308,6 +318,17 @@ hs_status hs_batch_get_field(hs_batch* b, int slot, double* T_host);
  * on the GPU race.  Do not call it on a device after cudaDeviceReset (the
  * cached address of the array is then stale). */
 hs_status hs_dot_noalloc(int N, const double* x, const double* y, double* out);
+
+/* A lognormal conductivity field of the reference generator's law
+ * (scripts/gen_field.py:29-61: white noise filtered to the periodic
+ * covariance exp(-r^2/L^2), standardised, k = exp(mu + sigma g)) generated on
+ * the current device into k_dev and rhoc_dev (N^3 doubles each, device;
+ * rhoc_dev is set to rhoc).  The filter is the real-space Gaussian kernel of
+ * the reference's Fourier filter, applied as three periodic 1-D passes; the
+ * noise is SplitMix64 of (seed, element) through Box-Muller.  Deterministic
+ * for given arguments; synchronous on the default stream. */
+hs_status hs_field_lognormal(int N, double mu, double sigma, double L, unsigned long long seed, double rhoc,
+                             double* k_dev, double* rhoc_dev);
 
 /* The reference solver's command line (het.cu:1340-1350, 1380-1433) with its
  * output files; returns the process exit code. */

@@ -26,7 +26,7 @@ EXPORTS = [
     "hs_arm_fi", "hs_run_case", "hs_verify", "hs_solve_host", "hs_diag_cg", "hs_set_dump", "hs_set_case_tag",
     "hs_target_on_boundary", "hs_classify", "hs_cli_main", "hs_advance", "hs_set_field", "hs_get_field",
     "hs_time_kernel", "hs_dot_noalloc", "hs_campaign", "hs_batch_default_options", "hs_batch_create",
-    "hs_batch_destroy", "hs_batch_add", "hs_batch_arm_flip", "hs_batch_arm_fault", "hs_batch_remove", "hs_batch_step",
+    "hs_batch_destroy", "hs_batch_add", "hs_batch_add_lognormal", "hs_field_lognormal", "hs_batch_arm_flip", "hs_batch_arm_fault", "hs_batch_remove", "hs_batch_step",
     "hs_batch_step_begin", "hs_batch_step_end", "hs_batch_info", "hs_batch_get_field", "hs_gaussian_ic",
 ]
 
@@ -165,6 +165,11 @@ def lib():
     L.hs_batch_destroy.argtypes = [vp]
     L.hs_batch_add.restype = i
     L.hs_batch_add.argtypes = [vp, i, C.c_double, vp, vp, vp, i, C.POINTER(i)]
+    L.hs_batch_add_lognormal.restype = i
+    L.hs_batch_add_lognormal.argtypes = [vp, i, C.c_double, C.c_double, C.c_double, C.c_double, C.c_ulonglong,
+                                         C.c_double, vp, i, C.POINTER(i)]
+    L.hs_field_lognormal.restype = i
+    L.hs_field_lognormal.argtypes = [i, C.c_double, C.c_double, C.c_double, C.c_ulonglong, C.c_double, vp, vp]
     L.hs_batch_arm_flip.restype = i
     L.hs_batch_arm_flip.argtypes = [vp, i, i, C.c_longlong, i]
     L.hs_batch_arm_fault.restype = i
@@ -413,6 +418,17 @@ class Batch:
         check(lib().hs_batch_create(C.byref(o), C.byref(self._h)))
         self.Nn = {}
 
+    def add_lognormal(self, N, dt, mu, sigma, L, seed, rhoc=1.0, T0=None, steps=1):
+        """An instance whose lognormal conductivity is generated on the device
+        (hs_batch_add_lognormal): no host field."""
+        T0 = None if T0 is None else _host(T0)
+        slot = C.c_int(-1)
+        check(lib().hs_batch_add_lognormal(self._h, int(N), float(dt), float(mu), float(sigma), float(L),
+                                           C.c_ulonglong(seed), float(rhoc),
+                                           T0.ctypes.data if T0 is not None else None, int(steps), C.byref(slot)))
+        self.Nn[slot.value] = (N + 1) ** 3
+        return slot.value
+
     def add(self, N, dt, k, rhoc, T0=None, steps=1):
         k, rhoc = _host(k), _host(rhoc)
         T0 = None if T0 is None else _host(T0)
@@ -482,6 +498,13 @@ def gaussian_ic(N, sigma=0.15):
     T = np.empty((N + 1) ** 3)
     check(lib().hs_gaussian_ic(int(N), float(sigma), T.ctypes.data))
     return T
+
+
+def field_lognormal(N, mu, sigma, L, seed, rhoc, k_dev, rhoc_dev):
+    """hs_field_lognormal: a lognormal conductivity field generated on the device
+    into the N^3-double device buffers at k_dev and rhoc_dev."""
+    check(lib().hs_field_lognormal(int(N), float(mu), float(sigma), float(L), C.c_ulonglong(seed), float(rhoc),
+                                   k_dev, rhoc_dev))
 
 
 def dot_noalloc(N, x_dev, y_dev, out_dev):

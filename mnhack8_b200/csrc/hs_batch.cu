@@ -341,16 +341,18 @@ void hs_batch_destroy(hs_batch* b) {
     delete b;
 }
 
-hs_status hs_batch_add(hs_batch* b, int N, double dt, const double* k, const double* rhoc, const double* T0,
-                       int n_steps, int* slot_out) {
-    if (!b || N < 1 || N > 1200 || !(dt > 0) || !k || !rhoc || n_steps < 0) {
-        set_error("hs_batch_add: bad arguments");
-        return HS_ERR_ARG;
-    }
+}  // extern "C"
+
+namespace {
+// An instance from host coefficient arrays (k, rhoc) or, when gen is set, from
+// a lognormal field generated on the device into the instance's arrays.
+hs_status batch_add_impl(hs_batch* b, int N, double dt, const double* k, const double* rhoc, const FieldSpecDev* gen,
+                         const double* T0, int n_steps, int* slot_out) {
     HS_CUDA(cudaSetDevice(b->opt.device));
     const long long NN = N + 1, Nn = NN * NN * NN, Ne = (long long)N * N * N;
-    for (long long e = 0; e < Ne; ++e)
-        if (!(k[e] > 0) || !(rhoc[e] > 0)) { set_error("hs_batch_add: non-positive coefficient"); return HS_ERR_ARG; }
+    if (!gen)
+        for (long long e = 0; e < Ne; ++e)
+            if (!(k[e] > 0) || !(rhoc[e] > 0)) { set_error("hs_batch_add: non-positive coefficient"); return HS_ERR_ARG; }
     const RefMatrices mats = build_reference_matrices(N);
     if (!mats.ok) { set_error("reference-matrix self-check failed"); return HS_ERR_MATRIX; }
     // slot
@@ -405,8 +407,16 @@ hs_status hs_batch_add(hs_batch* b, int N, double dt, const double* k, const dou
     d.st = b->d_st.p + slot;
     // coefficients (interleaved on the device), initial field
     const int gn = (int)std::min<long long>((Nn + RT - 1) / RT, 1 << 30);
-    HS_CUDA(cudaMemcpyAsync(rh, rhoc, Ne * 8, cudaMemcpyHostToDevice, sa));
-    HS_CUDA(cudaMemcpyAsync(kk, k, Ne * 8, cudaMemcpyHostToDevice, sa));
+    const long long nflat = (Nn + (long long)RT * KF - 1) / ((long long)RT * KF);
+    if (!b->sq.p) HS_CUDA(b->sq.alloc(4));
+    if (b->spart.n < (size_t)(2 * nflat)) HS_CUDA(b->spart.alloc(2 * nflat));   // s_add is its only user
+    if (gen) {
+        // the field on the device (the partials and the two moments reuse the set-up scratch)
+        HS_CUDA(enqueue_field_lognormal(*gen, kk, rh, b->spart.p, b->sq.p, sa));
+    } else {
+        HS_CUDA(cudaMemcpyAsync(rh, rhoc, Ne * 8, cudaMemcpyHostToDevice, sa));
+        HS_CUDA(cudaMemcpyAsync(kk, k, Ne * 8, cudaMemcpyHostToDevice, sa));
+    }
     if (T0) HS_CUDA(cudaMemcpyAsync(d.T, T0, Nn * 8, cudaMemcpyHostToDevice, sa));
     else HS_CUDA(cudaMemsetAsync(d.T, 0, Nn * 8, sa));
     k_pack_coef<<<grid_for(Ne, RT), RT, 0, sa>>>(Ne, rh, kk, (double2*)d.coef64, (float2*)d.coef32);
@@ -427,9 +437,6 @@ hs_status hs_batch_add(hs_batch* b, int N, double dt, const double* k, const dou
     k_apply_nodes<FORM_WHT><<<gn, RT, 0, sa>>>(gw);
     gw.dt_eff = dt; gw.y = wA;
     k_apply_nodes<FORM_WHT><<<gn, RT, 0, sa>>>(gw);
-    const long long nflat = (Nn + (long long)RT * KF - 1) / ((long long)RT * KF);
-    if (!b->sq.p) HS_CUDA(b->sq.alloc(4));
-    if (b->spart.n < (size_t)(2 * nflat)) HS_CUDA(b->spart.alloc(2 * nflat));   // s_add is its only user
     RedArgs r1{Nn, nflat, N, RED_DOT, wM, wM, b->spart.p, nullptr, nullptr};
     k_reduce<<<(int)nflat, RT, 0, sa>>>(r1);
     k_final_reduce<<<1, RT, 0, sa>>>(b->spart.p, nflat, b->sq.p);
@@ -448,6 +455,28 @@ hs_status hs_batch_add(hs_batch* b, int N, double dt, const double* k, const dou
     b->dirty = true;
     if (slot_out) *slot_out = slot;
     return HS_OK;
+}
+}  // namespace
+
+extern "C" {
+
+hs_status hs_batch_add(hs_batch* b, int N, double dt, const double* k, const double* rhoc, const double* T0,
+                       int n_steps, int* slot_out) {
+    if (!b || N < 1 || N > 1200 || !(dt > 0) || !k || !rhoc || n_steps < 0) {
+        set_error("hs_batch_add: bad arguments");
+        return HS_ERR_ARG;
+    }
+    return batch_add_impl(b, N, dt, k, rhoc, nullptr, T0, n_steps, slot_out);
+}
+
+hs_status hs_batch_add_lognormal(hs_batch* b, int N, double dt, double mu, double sigma, double L,
+                                 unsigned long long seed, double rhoc, const double* T0, int n_steps, int* slot_out) {
+    if (!b || N < 1 || N > 1200 || !(dt > 0) || !(sigma >= 0) || !(L > 0) || !(rhoc > 0) || n_steps < 0) {
+        set_error("hs_batch_add_lognormal: bad arguments");
+        return HS_ERR_ARG;
+    }
+    const FieldSpecDev f{N, mu, sigma, L, rhoc, seed};
+    return batch_add_impl(b, N, dt, nullptr, nullptr, &f, T0, n_steps, slot_out);
 }
 
 hs_status hs_batch_arm_flip(hs_batch* b, int slot, int step, long long idx, int bit) {

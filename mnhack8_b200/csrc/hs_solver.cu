@@ -1090,5 +1090,7 @@ hs_status hs_time_kernel(hs_solver* h, int which, int reps, double* ms_per_launc
 #include "hs_noalloc.cu"
 // the fault-injection campaign resumes trajectories through run_case_impl
 #include "hs_campaign.cu"
+// lognormal fields generated on the device (standalone and for batched instances)
+#include "hs_field.cu"
 // the batched mixed-precision solver reuses the slab partition and set-up kernels
 #include "hs_batch.cu"
