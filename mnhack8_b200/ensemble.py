@@ -202,7 +202,12 @@ def request_stream(n, rate, seed, nmin=16, nmax=160, smin=10, smax=100, flip_fra
     return reqs
 
 
-def serving(n=400, rate=200.0, seed=11, rtol=1e-8, inner_tol=1e-4, max_live=64, hbm_fraction=0.5, device=0):
+def serving(n=400, rate=200.0, seed=11, rtol=1e-8, inner_tol=1e-4, max_live=64, hbm_fraction=0.5, device=0,
+            gpu_fields=False):
+    """gpu_fields: the batched server generates each request's field on the
+    device when it admits the request (hs_batch_add_lognormal), so the field's
+    generation is inside the served latency; the serial FP64 side keeps the
+    host fields generated before its timed region."""
     import torch
     import concurrent.futures as cf
     import multiprocessing as mp
@@ -236,7 +241,10 @@ def serving(n=400, rate=200.0, seed=11, rtol=1e-8, inner_tol=1e-4, max_live=64, 
                live_bytes + batch_bytes(queue[0]["N"]) <= budget):
             q = queue.pop(0)
             live_bytes += batch_bytes(q["N"])
-            s = b.add(q["N"], DT, q["k"], q["r"], T0=q["T0"], steps=q["steps"])
+            if gpu_fields:
+                s = b.add_lognormal(q["N"], DT, 0.0, 1.0, 1.0 / 8.0, q["seed"], rhoc=1.0, T0=q["T0"], steps=q["steps"])
+            else:
+                s = b.add(q["N"], DT, q["k"], q["r"], T0=q["T0"], steps=q["steps"])
             if q["flip"]:
                 b.arm_flip(s, *q["flip"])
             q["left"] = q["steps"]
@@ -306,6 +314,8 @@ def serving(n=400, rate=200.0, seed=11, rtol=1e-8, inner_tol=1e-4, max_live=64, 
                         "p99_latency_s": pct(lat_s, 99), "handle_setup_s_total": create_s,
                         "handle_setup_s_per_request": create_s / n},
         "throughput_ratio": (n / wall_b) / (n / wall_s),
+        "batched_fields": "device, at admission, inside the timed stream" if gpu_fields else
+                          "host, before the stream",
         "field_generation": {"where": "host, the reference generator's FFT algorithm (NumPy), before the stream",
                              "per_request_mean_s": float(np.mean(gen_each)),
                              "per_request_p99_s": float(np.percentile(gen_each, 99)),
@@ -449,6 +459,7 @@ def _main(argv=None):
     p.add_argument("--N", type=int, default=128)
     p.add_argument("--steps", type=int, default=2)
     p = sub.add_parser("serving")
+    p.add_argument("--gpu-fields", action="store_true")
     p.add_argument("--n", type=int, default=400)
     p.add_argument("--rate", type=float, default=200.0)
     p.add_argument("--max-live", type=int, default=64)
@@ -462,7 +473,7 @@ def _main(argv=None):
     elif a.cmd == "single":
         out = single(N=a.N, steps=a.steps)
     else:
-        out = serving(n=a.n, rate=a.rate, max_live=a.max_live)
+        out = serving(n=a.n, rate=a.rate, max_live=a.max_live, gpu_fields=a.gpu_fields)
     print(json.dumps(out), flush=True)
     return 0
 
