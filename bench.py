@@ -385,6 +385,8 @@ def main():
     }
     if rank == 0 and not args.no_gate and N != GATE_N:
         line["apply_gate_N256"] = gate_apply(local, detect, args.kernel, args.scatter)
+    if rank == 0 and args.scatter == "colored":
+        line["scatter_pair"] = scatter_pair(N, local, detect, args.kernel, ms_k1)
     if rank == 0 and world == 1 and args.batching_instances > 0:
         line["batching"] = batching_leg(args.batching_instances, local)
     if rank == 0 and world == 1 and args.serving_requests > 0:
@@ -466,6 +468,22 @@ def gate_apply(device, detect, kernel, scatter):
     ach = alg / (ms * 1e-3) / 1e9
     return {"N": N, "ms_per_launch": ms, "alg_bytes_per_launch": alg, "achieved": ach, "peak": peak,
             "unit": "GB/s", "frac": ach / peak, "peak_source": f"{kind} hbm_gbs", "l2": "flushed before each launch"}
+
+
+def scatter_pair(N, device, detect, kernel, ms_colored):
+    """Supplementary (config 2's comparison): the PCG operator per application
+    with the atomic scatter (p formation, zeroing, element bricks with shared-
+    memory accumulation and global atomics on brick faces, projection and
+    partials) beside the colored kernel, same field, L2 scrubbed."""
+    from mnhack8_b200 import _lib
+    k, r = make_field(N, 1)
+    g = _lib.Solver(N, DT, k, r, kernel=kernel, scatter="atomic", detect=detect, no_source=True, ic="gaussian",
+                    ic_sigma=IC_SIGMA, rtol=RTOL, max_iter=500, device=device)
+    g.time_kernel(0, reps=3)
+    ms = g.time_kernel(0, reps=20)
+    g.close()
+    return {"N": N, "colored_ms_per_apply": ms_colored, "atomic_ms_per_apply": ms,
+            "atomic_over_colored": ms / ms_colored}
 
 
 def _initial(g, N):

@@ -721,8 +721,18 @@ struct AtomArgs {
     const DevState* st;
     ElemConsts ec;
 };
+// Bricks of AB_X x AB_Y x AB_Z elements, one element per thread: the element
+// outputs are added into the brick's node block in shared memory (shared
+// atomics), and only the nodes on the brick's faces, which neighbouring
+// bricks also touch, are added to y with global atomics; the brick's inner
+// nodes are stored.  y is zeroed beforehand.  The order of the additions is
+// not fixed (the reference's atomic mode is not bit-reproducible either).
+constexpr int AB_X = 4, AB_Y = 8, AB_Z = 8;
+constexpr int AB_NODES = (AB_X + 1) * (AB_Y + 1) * (AB_Z + 1);
 template <int FORM>
 __global__ void __launch_bounds__(RT) k_apply_atomic(AtomArgs a) {
+    static_assert(AB_X * AB_Y * AB_Z == RT, "one element per thread");
+    __shared__ double acc[AB_NODES];
     const DevState* st = a.st;
     const double* x = a.x;
     if (a.role == ROLE_LOOP) {
@@ -731,21 +741,38 @@ __global__ void __launch_bounds__(RT) k_apply_atomic(AtomArgs a) {
     }
     const bool fire_r = (a.role == ROLE_X0) && st->fi_armR;
     const int N = a.N;
-    const long long NN = N + 1, Ne = (long long)N * N * N;
-    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= Ne) return;
-    const int ex = (int)(e / ((long long)N * N)), ey = (int)((e / N) % N), ez = (int)(e % N);
-    double v[8];
-    long long g[8];
+    const long long NN = N + 1;
+    const int nbz = (N + AB_Z - 1) / AB_Z, nby = (N + AB_Y - 1) / AB_Y;
+    const int bz = blockIdx.x % nbz, by = (blockIdx.x / nbz) % nby, bx = blockIdx.x / (nbz * nby);
+    const int x0 = bx * AB_X, y0 = by * AB_Y, z0 = bz * AB_Z;
+    for (int i = threadIdx.x; i < AB_NODES; i += RT) acc[i] = 0.0;
+    __syncthreads();
+    const int tz = threadIdx.x % AB_Z, ty = (threadIdx.x / AB_Z) % AB_Y, tx = threadIdx.x / (AB_Z * AB_Y);
+    const int ex = x0 + tx, ey = y0 + ty, ez = z0 + tz;
+    if (ex < N && ey < N && ez < N) {
+        const long long e = ((long long)ex * N + ey) * N + ez;
+        double v[8];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        g[q] = ((long long)(ex + ((q >> 2) & 1)) * NN + ey + ((q >> 1) & 1)) * NN + ez + (q & 1);
-        v[q] = __ldg(x + g[q]);
+        for (int q = 0; q < 8; ++q)
+            v[q] = __ldg(x + ((long long)(ex + ((q >> 2) & 1)) * NN + ey + ((q >> 1) & 1)) * NN + ez + (q & 1));
+        elem_apply<FORM>(v, __ldg(a.rhoc + e), __ldg(a.kc + e), a.dt_eff, a.ec);
+        if (fire_r && e == st->fi_elem) v[0] = flipbit(v[0], st->fi_bit);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int lx = tx + ((q >> 2) & 1), ly = ty + ((q >> 1) & 1), lz = tz + (q & 1);
+            atomicAdd(&acc[(lx * (AB_Y + 1) + ly) * (AB_Z + 1) + lz], v[q]);
+        }
     }
-    elem_apply<FORM>(v, __ldg(a.rhoc + e), __ldg(a.kc + e), a.dt_eff, a.ec);
-    if (fire_r && e == st->fi_elem) v[0] = flipbit(v[0], st->fi_bit);
-#pragma unroll
-    for (int q = 0; q < 8; ++q) atomicAdd(a.y + g[q], v[q]);
+    __syncthreads();
+    for (int i = threadIdx.x; i < AB_NODES; i += RT) {
+        const int lz = i % (AB_Z + 1), ly = (i / (AB_Z + 1)) % (AB_Y + 1), lx = i / ((AB_Z + 1) * (AB_Y + 1));
+        const int gx = x0 + lx, gy = y0 + ly, gz = z0 + lz;
+        if (gx > N || gy > N || gz > N) continue;
+        const long long n = ((long long)gx * NN + gy) * NN + gz;
+        const bool face = lx == 0 || lx == AB_X || ly == 0 || ly == AB_Y || lz == 0 || lz == AB_Z;
+        if (face) atomicAdd(a.y + n, acc[i]);
+        else a.y[n] = acc[i];
+    }
 }
 
 // After an atomic scatter: projection, p.Ap / D1 partials and role logic, on

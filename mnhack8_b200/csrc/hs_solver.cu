@@ -161,7 +161,8 @@ void launch_nodes(hs_solver* h, const GenArgs& a) {
     }
 }
 void launch_atomic(hs_solver* h, const AtomArgs& a) {
-    const int g = grid_for(h->Ne, RT, 1 << 30);
+    const int N = h->N;
+    const int g = ((N + AB_X - 1) / AB_X) * ((N + AB_Y - 1) / AB_Y) * ((N + AB_Z - 1) / AB_Z);
     switch (h->opt.kernel) {
         case HS_KERNEL_WHT: k_apply_atomic<FORM_WHT><<<g, RT, 0, h->s>>>(a); break;
         case HS_KERNEL_GAUSS: k_apply_atomic<FORM_GAUSS><<<g, RT, 0, h->s>>>(a); break;
