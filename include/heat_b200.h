@@ -247,8 +247,8 @@ typedef struct hs_batch_options {
     int max_outer;        /* corrections per step */
     int max_inner;        /* inner PCG iterations per correction */
     int detect;           /* ABFT checksum on every operator apply */
-    int tile_planes;      /* operator tiles span min(N+1, tile_planes) planes; 0: a depth set by N
-                             alone (the instance by itself fills the GPU, within 8..32 planes) */
+    int tile_planes;      /* operator x-slabs span min(N+1, tile_planes) planes; 0: a depth set by N
+                             alone (the single-instance choice when >= 16 planes, else 16) */
     int device;
     int extrapolate;      /* start each step (after the first) from 2 T - T_prev instead of T */
 } hs_batch_options;

@@ -5,6 +5,7 @@ heat_solver_b200's entry point.  The files the reference's validation scripts
 parse carry the reference's recorded values to their printed digits (E(t)
 to its 11 digits within one unit of the last)."""
 import csv
+import math
 import os
 
 import numpy as np
@@ -36,8 +37,9 @@ def test_v6_level_R_case_through_the_cli(tmp_path, golden):
             assert got[key] == want[key], (want["step"], key)
         # E(t): 11 printed digits, the last within one unit (the recorded run
         # summed its reductions in another order; E is a difference of two runs)
-        assert abs(float(got["E_fault"]) - float(want["E_fault"])) <= 5e-11 * abs(float(want["E_fault"])), \
-            (want["step"], got["E_fault"], want["E_fault"])
+        w = float(want["E_fault"])
+        unit = 10.0 ** (math.floor(math.log10(abs(w))) - 10) if w else 0.0
+        assert abs(float(got["E_fault"]) - w) <= 1.5 * unit, (want["step"], got["E_fault"], want["E_fault"])
         if want["step"] == sm["fi_step"]:
             assert got["d1_abft_F"] == want["d1_abft_F"]
     with open(out / "fi_summary_det.csv") as f:

@@ -112,7 +112,8 @@ def test_v6_level_R_bit55(ln32_runs, golden, oracle):
         # 11 printed digits; the last may differ by one, as the recorded run's
         # reductions summed in another order (E is a difference of two runs)
         want = float(gt["E_fault"])
-        assert abs(x["E"] - want) <= 5e-11 * abs(want), (gt["step"], gt["E_fault"], x["E"])
+        unit = 10.0 ** (math.floor(math.log10(abs(want))) - 10) if want else 0.0
+        assert abs(x["E"] - want) <= 1.5 * unit, (gt["step"], gt["E_fault"], x["E"])
         assert gt["spread_F"] == "%.4f" % x["spread"]
         assert int(gt["cg_F"]) == x["cg_iters"]
         assert gt["d2_resid_F"] == "%.3e" % x["d2"]
