@@ -325,7 +325,7 @@ def serving(n=400, rate=200.0, seed=11, rtol=1e-8, inner_tol=1e-4, max_live=64, 
 
 
 # ---- config 3: detection coverage of the mixed form, beside FP64 ------------------------
-def coverage(N=64, steps=20, flips=1000, seed=21, per_batch=125, rtol=1e-8, inner_tol=1e-4, sigma=1.5,
+def coverage(N=64, steps=20, flips=1000, seed=21, per_batch=None, rtol=1e-8, inner_tol=1e-4, sigma=1.5,
              corr_frac=1.0 / 16.0, sig_err=1e-6, device=0, rows_out=None, fp64=True):
     """Seeded single-bit flips into the FP32 inner vectors of the mixed form
     (p after formation, r after its update, Ap after projection; bits 0..31,
@@ -348,6 +348,11 @@ def coverage(N=64, steps=20, flips=1000, seed=21, per_batch=125, rtol=1e-8, inne
     T_clean, clean = b.field(s), b.info(s)
     b.close()
     thr32 = max(100.0 * clean["d1_max32"], 1e-12)
+    if per_batch is None:
+        # faulted copies per batch: at most 125, within 60 % of the free HBM
+        import torch
+        free, _ = torch.cuda.mem_get_info(device)
+        per_batch = int(max(1, min(125, 0.6 * free // batch_bytes(N))))
     per_corr = max(1, int(clean["inner_iters"] / max(1, clean["outer_iters"])))
     rng = np.random.default_rng(seed)
     sites = [dict(level=int(rng.choice([5, 6, 7])), step=int(rng.integers(0, steps)), outer=1,
@@ -452,6 +457,7 @@ def _main(argv=None):
     p.add_argument("--serial-sample", type=int, default=None)
     p = sub.add_parser("coverage")
     p.add_argument("--N", type=int, default=64)
+    p.add_argument("--steps", type=int, default=20)
     p.add_argument("--flips", type=int, default=1000)
     p.add_argument("--rows", default=None, help="write the mixed form's per-flip rows (JSON) here")
     p.add_argument("--no-fp64", action="store_true")
@@ -467,7 +473,7 @@ def _main(argv=None):
     if a.cmd == "precision":
         out = precision(N=a.N, steps=a.steps)
     elif a.cmd == "coverage":
-        out = coverage(N=a.N, flips=a.flips, rows_out=a.rows, fp64=not a.no_fp64)
+        out = coverage(N=a.N, steps=a.steps, flips=a.flips, rows_out=a.rows, fp64=not a.no_fp64)
     elif a.cmd == "batching":
         out = batching(n=a.n, steps=a.steps, serial_sample=a.serial_sample)
     elif a.cmd == "single":
