@@ -22,8 +22,10 @@
 //   3. the element operator, then the node sum of node (x, r-1, c) in the
 //      canonical order 4, 7, 6, 5 (from layer x-1, kept as a "lower" sum) and
 //      0, 3, 2, 1 (this layer), projection, p.Ap / D1 partials and the store.
-// The inputs of step i+2 are loaded during step i (three rotating register
-// sets), so every load has two steps of work to arrive.
+// The inputs of layer x+1 are copied into shared memory while layer x runs
+// (asynchronous 8-byte copies, cp.async, into per-lane slots of a two-layer
+// ring), so a load has a whole layer of work to arrive and costs no register
+// until it is used; a lane reads only its own slots, so no barrier is needed.
 //
 // Elements outside the domain (the first lane of the first segment, column
 // -1; the element column N of the lane owning node column N; element rows -1
@@ -65,18 +67,28 @@ __device__ __forceinline__ ColLane col_lane(const ColLayout& L, long long wt, in
     return c;
 }
 
-// inputs of one step: node row (columns c, c+1) of the formed plane, its ABFT
-// weight, and the coefficients of the element below the row
-struct ColStep {
-    double a0, a1, b0, b1, w, cr, ck;
-};
-
 __device__ __forceinline__ double shfl_up1(double v) { return __shfl_up_sync(0xffffffffu, v, 1); }
+
+// asynchronous 8-byte global -> shared copy; valid == false reads nothing and
+// writes zeros (source size 0)
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem, bool valid) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    const int nbytes = valid ? 8 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(nbytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prior1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+// fields of one step in the shared-memory ring (one double per lane each)
+enum ColField { CF_A0 = 0, CF_A1, CF_B0, CF_B1, CF_W, CF_CR, CF_CK, CF_N };
+constexpr int kColSteps = CR + 2;
+// ring: [layer parity][step][field][RT threads]
+constexpr size_t kColSmem = (size_t)2 * kColSteps * CF_N * RT * sizeof(double);
 
 // MODE 0: input x as given; 1: PCG loop, p = z; 2: PCG loop, p = z + beta p_{k-1}.
 // FI false: no fault is armed for this launch (the fault tests compile out).
 template <int FORM, int MODE, bool FI>
-__device__ __forceinline__ void col_march(const ApplyArgs& a, const ColLane& C, const double* srcA,
+__device__ __forceinline__ void col_march(const ApplyArgs& a, const ColLane& C, double* ring, const double* srcA,
                                           const double* srcB, double beta, double* pout, bool loop, bool d1,
                                           bool rhs, int fi_p, int fi_ap, int fi_r, int fi_bit, long long fi_idx,
                                           long long fi_elem, double (&part)[MAXQ]) {
@@ -104,22 +116,33 @@ __device__ __forceinline__ void col_march(const ApplyArgs& a, const ColLane& C, 
     const int lane_n = (r0 - 1) * NN + ec;             // node index offset of row r0-1, column c
     const int lane_e = (r0 - 2) * N + ec;              // element index offset of row r0-2, column c
 
-    auto load = [&](ColStep& B, int x, int i) {
+    const int tid = threadIdx.x;
+    // copies of layer x's inputs (plane x+1 rows, coefficients of layer x) into ring half par
+    auto issue_layer = [&](int x, int par) {
         const int xp = x + 1;
-        const bool pv = xp >= 0 && xp <= N && xp <= xb + 1 && ((rowv >> i) & 1u);
-        const int n = xp * NN * NN + lane_n + i * NN;
-        const bool v0 = pv && colv, v1 = pv && colv1;
-        B.a0 = v0 ? __ldg(srcA + n) : 0.0;
-        B.a1 = v1 ? __ldg(srcA + n + 1) : 0.0;
-        if (MODE == 2) {
-            B.b0 = v0 ? __ldg(srcB + n) : 0.0;
-            B.b1 = v1 ? __ldg(srcB + n + 1) : 0.0;
+        const bool plane_ok = xp >= 0 && xp <= N && xp <= xb + 1;
+        const bool w_ok = d1 && xp >= xa && xp <= xb;
+        const bool el_ok = x >= xa - 1 && x >= 0 && x < N && ecv;
+#pragma unroll
+        for (int i = 0; i < NS; ++i) {
+            double* slot = ring + ((size_t)(par * NS + i) * CF_N) * RT + tid;
+            const bool pv = plane_ok && ((rowv >> i) & 1u);
+            const int n = xp * NN * NN + lane_n + i * NN;
+            const bool v0 = pv && colv, v1 = pv && colv1;
+            cp_async8(slot + CF_A0 * RT, v0 ? srcA + n : srcA, v0);
+            cp_async8(slot + CF_A1 * RT, v1 ? srcA + n + 1 : srcA, v1);
+            if (MODE == 2) {
+                cp_async8(slot + CF_B0 * RT, v0 ? srcB + n : srcB, v0);
+                cp_async8(slot + CF_B1 * RT, v1 ? srcB + n + 1 : srcB, v1);
+            }
+            const bool wv = w_ok && v0 && ((orow >> i) & 1u);
+            cp_async8(slot + CF_W * RT, wv ? a.w + n : a.y, wv);
+            const bool ev = i >= 1 && el_ok && ((erowv >> i) & 1u);
+            const double* ce = reinterpret_cast<const double*>(a.coef) + 2 * (long long)(x * N * N + lane_e + i * N);
+            cp_async8(slot + CF_CR * RT, ev ? ce : srcA, ev);
+            cp_async8(slot + CF_CK * RT, ev ? ce + 1 : srcA, ev);
         }
-        B.w = (d1 && v0 && xp >= xa && xp <= xb && ((orow >> i) & 1u)) ? __ldg(a.w + n) : 0.0;
-        const bool ev = i >= 1 && x >= xa - 1 && x >= 0 && x < N && ecv && ((erowv >> i) & 1u);
-        const double2 c = ev ? __ldg(a.coef + (x * N * N + lane_e + i * N)) : make_double2(0.0, 0.0);
-        B.cr = c.x;
-        B.ck = c.y;
+        cp_async_commit();
     };
 
     double fp[CR + 1][4];     // wht: y-butterflied faces of plane x, element rows r0-1+j
@@ -133,10 +156,7 @@ __device__ __forceinline__ void col_march(const ApplyArgs& a, const ColLane& C, 
     }
 #pragma unroll
     for (int i = 0; i < NS; ++i) pl[i][0] = pl[i][1] = 0.0;
-    ColStep B0, B1, B2;
-    B0.b0 = B0.b1 = B1.b0 = B1.b1 = B2.b0 = B2.b1 = 0.0;
-    load(B0, xa - 2, 0);
-    load(B1, xa - 2, 1);
+    issue_layer(xa - 2, 0);
 
     // layer xa-2 only forms plane xa-1 (the slab's lower halo plane); layers
     // xa-1 .. xb apply their elements
@@ -147,15 +167,18 @@ __device__ __forceinline__ void col_march(const ApplyArgs& a, const ColLane& C, 
         double zsP_s = 0.0, zsP_d = 0.0;       // z butterfly of the previous row
         double pnA = 0.0, pnB = 0.0;           // p of the previous row (plane x+1)
         double hq2 = 0.0, hL3 = 0.0, hq6 = 0.0, hL7 = 0.0;   // element row below: its oy = 1 outputs
+        const int par = (x - xa) & 1;          // ring half of this layer (layer xa-2 is half 0)
+        // the next layer's inputs go out now; this layer's have arrived once at most one group is pending
+        if (x + 1 <= xb) issue_layer(x + 1, par ^ 1);
+        else cp_async_commit();                // an empty group keeps the count
+        cp_async_wait_prior1();
+        const double* lring = ring + ((size_t)par * NS * CF_N) * RT + tid;
 #pragma unroll
         for (int i = 0; i < NS; ++i) {
-            ColStep& B = (i % 3 == 0) ? B0 : (i % 3 == 1) ? B1 : B2;
-            const double a0 = B.a0, a1 = B.a1, b0 = B.b0, b1 = B.b1, wv = B.w, cr = B.cr, ck = B.ck;
-            {   // inputs of step i+2 (the next layer's first steps at the end of this one)
-                ColStep& BL = ((i + 2) % 3 == 0) ? B0 : ((i + 2) % 3 == 1) ? B1 : B2;
-                if (i + 2 < NS) load(BL, x, i + 2);
-                else load(BL, x + 1, i + 2 - NS);
-            }
+            const double* sl = lring + (size_t)i * CF_N * RT;
+            const double a0 = sl[CF_A0 * RT], a1 = sl[CF_A1 * RT];
+            const double b0 = (MODE == 2) ? sl[CF_B0 * RT] : 0.0, b1 = (MODE == 2) ? sl[CF_B1 * RT] : 0.0;
+            const double wv = sl[CF_W * RT], cr = sl[CF_CR * RT], ck = sl[CF_CK * RT];
             const int r = r0 - 1 + i;                   // node row formed, plane x+1
             // 1. p at (x+1, r, c) and (x+1, r, c+1)
             double pA, pB;
@@ -259,11 +282,11 @@ __device__ __forceinline__ void col_march(const ApplyArgs& a, const ColLane& C, 
 
 // Colored operator on the COL partition: tile blockIdx.x (CW warp tasks).
 // LOOP: the PCG-loop role (p formed in the kernel); otherwise the roles that
-// apply the operator to a given vector.  One tile per SM: a lane keeps its
-// rows' faces, lower sums and two steps of loads in registers (about 220).
+// apply the operator to a given vector.  One tile per SM (the 172 KB ring).
 template <int FORM, bool LOOP>
 __global__ void __launch_bounds__(RT, 1) k_apply_col(ApplyArgs a) {
     __shared__ double sh[MAXQ][8];
+    extern __shared__ __align__(16) double col_ring[];     // kColSmem bytes
     DevState* st = a.st;
     int fi_p = 0, fi_ap = 0, fi_r = 0, fi_bit = 0;
     long long fi_idx = -1, fi_elem = -1;
@@ -284,23 +307,23 @@ __global__ void __launch_bounds__(RT, 1) k_apply_col(ApplyArgs a) {
         }
         if (wlive) {
             if (!src_b)
-                col_march<FORM, 1, true>(a, C, a.z, nullptr, 0.0, pout, true, d1, false, fi_p, fi_ap, 0, fi_bit,
+                col_march<FORM, 1, true>(a, C, col_ring, a.z, nullptr, 0.0, pout, true, d1, false, fi_p, fi_ap, 0, fi_bit,
                                          fi_idx, -1, part);
             else if (fi_p || fi_ap)
-                col_march<FORM, 2, true>(a, C, a.z, src_b, beta, pout, true, d1, false, fi_p, fi_ap, 0, fi_bit,
+                col_march<FORM, 2, true>(a, C, col_ring, a.z, src_b, beta, pout, true, d1, false, fi_p, fi_ap, 0, fi_bit,
                                          fi_idx, -1, part);
             else
-                col_march<FORM, 2, false>(a, C, a.z, src_b, beta, pout, true, d1, false, 0, 0, 0, 0, -1, -1, part);
+                col_march<FORM, 2, false>(a, C, col_ring, a.z, src_b, beta, pout, true, d1, false, 0, 0, 0, 0, -1, -1, part);
         }
     } else {
         if (a.role == ROLE_X0 && st->fi_armR) { fi_r = 1; fi_elem = st->fi_elem; fi_bit = st->fi_bit; }
         const bool rhs = (a.role == ROLE_RHS) && a.F != nullptr;
         if (wlive) {
             if (fi_r)
-                col_march<FORM, 0, true>(a, C, a.x, nullptr, 0.0, nullptr, false, d1, rhs, 0, 0, 1, fi_bit, -1,
+                col_march<FORM, 0, true>(a, C, col_ring, a.x, nullptr, 0.0, nullptr, false, d1, rhs, 0, 0, 1, fi_bit, -1,
                                          fi_elem, part);
             else
-                col_march<FORM, 0, false>(a, C, a.x, nullptr, 0.0, nullptr, false, d1, rhs, 0, 0, 0, 0, -1, -1,
+                col_march<FORM, 0, false>(a, C, col_ring, a.x, nullptr, 0.0, nullptr, false, d1, rhs, 0, 0, 0, 0, -1, -1,
                                           part);
         }
         if (!d1) return;

@@ -140,10 +140,26 @@ int nblocks(const hs_solver* h) { return (int)h->cp.ntiles; }
 
 // ---- operator launches -------------------------------------------------------------
 template <int FORM>
+bool set_col_smem() {
+    return cudaFuncSetAttribute(k_apply_col<FORM, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kColSmem) == cudaSuccess &&
+           cudaFuncSetAttribute(k_apply_col<FORM, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kColSmem) == cudaSuccess;
+}
+// the operator kernel's input ring exceeds the default 48 KB of dynamic shared memory
+bool set_smem_attributes() {
+    static bool done = false, ok = true;
+    if (done) return ok;
+    done = true;
+    ok = set_col_smem<FORM_WHT>() && set_col_smem<FORM_FAST>() && set_col_smem<FORM_GAUSS>();
+    return ok;
+}
+
+template <int FORM>
 void launch_col(hs_solver* h, const ApplyArgs& a) {
     const int g = (int)h->cp.ntiles;
-    if (a.role == ROLE_LOOP) k_apply_col<FORM, true><<<g, RT, 0, h->s>>>(a);
-    else k_apply_col<FORM, false><<<g, RT, 0, h->s>>>(a);
+    if (a.role == ROLE_LOOP) k_apply_col<FORM, true><<<g, RT, kColSmem, h->s>>>(a);
+    else k_apply_col<FORM, false><<<g, RT, kColSmem, h->s>>>(a);
 }
 void launch_colored(hs_solver* h, const ApplyArgs& a) {
     switch (h->opt.kernel) {
@@ -398,6 +414,7 @@ hs_status hs_create(const hs_options* opt, const double* k_host, const double* r
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { set_error("No CUDA devices"); return HS_ERR_CUDA; }
     HS_CUDA(cudaSetDevice(opt->device % ndev));
+    if (!set_smem_attributes()) { set_error("cannot raise the shared-memory limit of the operator kernel"); return HS_ERR_CUDA; }
     std::unique_ptr<hs_solver> h(new hs_solver());
     h->opt = *opt;
     const int N = opt->N;
