@@ -390,17 +390,15 @@ __device__ __forceinline__ void update_scalars(const UpdateArgs& a, const double
 // p.Ap is the same bits everywhere), and CTA 0 records p.Ap, alpha, the D1
 // checksum and a breakdown.
 //
-// It also finishes its own reductions.  The FLAT order's final pass gives
-// thread l of its block tree the partials of blocks l, l+RT, l+2RT, ... added
-// in that order; the kernel runs exactly RT CTAs and CTA c visits the blocks
-// c, c+RT, ... in increasing order (two at a time), so CTA c forms thread c's
-// sequential sum itself.  The last CTA to finish (an atomic ticket) combines
-// the RT sums with the block tree and runs the scalar logic.
-constexpr int kUpdateCtas = RT;
-__global__ void __launch_bounds__(RT, 2) k_update(UpdateArgs a) {
+// It also finishes its own reductions: each flat block's partials are stored
+// at the block's index, and the last CTA to finish (an atomic ticket) combines
+// them in the FLAT order (final_sums) and runs the scalar logic, the work a
+// separate single-CTA kernel would do after it.
+constexpr int kUpdateCtasPerSm = 5;
+__global__ void __launch_bounds__(RT, kUpdateCtasPerSm) k_update(UpdateArgs a) {
     static_assert(KF % 2 == 0, "pairs of nodes per thread");
     constexpr int NC = KF / 2;
-    __shared__ double sh[6][8];
+    __shared__ double sh[MAXQ][8];
     __shared__ double s_pAp;
     __shared__ unsigned s_last;
     DevState* st = a.st;
@@ -509,38 +507,27 @@ __global__ void __launch_bounds__(RT, 2) k_update(UpdateArgs a) {
             stv(a.x, xx); stv(a.r, rr); stv(a.z, dd);
         }
     };
-    // this CTA's strided sequential sums (thread blockIdx.x of the final pass), in thread 0
-    double seq[3] = {0.0, 0.0, 0.0};
-    const long long G = gridDim.x;
-    for (long long b0 = blockIdx.x; b0 < a.nflat; b0 += 2 * G) {
-        double part[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-        block(b0, part);
-        block(b0 + G, part + 3);
-        cta_tree_sum<6>(part, sh);
+    // flat blocks blockIdx.x, + gridDim.x, ...; each block's partials at its own index
+    for (long long blk = blockIdx.x; blk < a.nflat; blk += gridDim.x) {
+        double part[3] = {0.0, 0.0, 0.0};
+        block(blk, part);
+        cta_tree_sum<3>(part, sh);
         if (tid == 0) {
 #pragma unroll
-            for (int q = 0; q < 3; ++q) seq[q] = dadd(seq[q], part[q]);
-            if (b0 + G < a.nflat) {
-#pragma unroll
-                for (int q = 0; q < 3; ++q) seq[q] = dadd(seq[q], part[3 + q]);
-            }
+            for (int q = 0; q < 3; ++q) a.partials[q * a.nflat + blk] = part[q];
         }
     }
     if (tid == 0) {
-#pragma unroll
-        for (int q = 0; q < 3; ++q) a.partials[q * RT + blockIdx.x] = seq[q];
         __threadfence();
         const unsigned t = atomicAdd(a.ticket, 1u);
         s_last = (t == gridDim.x - 1) ? 1u : 0u;
     }
     __syncthreads();
     if (!s_last) return;
-    // the last CTA: block tree over the RT sums, then the scalar logic
+    // the last CTA: the FLAT order's final combination, then the scalar logic
     __threadfence();
     double v[3];
-#pragma unroll
-    for (int q = 0; q < 3; ++q) v[q] = __ldcg(a.partials + q * RT + tid);
-    cta_tree_sum<3>(v, sh);
+    final_sums<3, 4>(v, a.partials, a.nflat, sh);     // short load batches keep the registers low
     if (tid == 0) {
         *a.ticket = 0u;
         update_scalars(a, v);

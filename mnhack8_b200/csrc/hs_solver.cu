@@ -86,7 +86,7 @@ struct hs_solver {
     DevBuf<double> diag, F, wM, wA;
     DevBuf<double> T, b, r, z, p0, p1, Ap;
     DevBuf<double> partials;            // operator tiles (and the standalone reductions)
-    DevBuf<double> upart;               // PCG vector update: per-CTA strided sums of its block partials
+    DevBuf<double> upart;               // PCG vector update: per-block partials (FLAT order)
     int n_sm = 148;
     DevBuf<unsigned> ticket;
     DevBuf<DevState> st;
@@ -235,8 +235,9 @@ void launch_update(hs_solver* h, int role, bool use_cond, cudaGraphConditionalHa
     u.st = h->st.p; u.cond = cond; u.use_cond = 0;
     u.d1 = h->opt.detect != 0; u.apart = h->partials.p; u.nblk = h->cp.ntiles;
     u.cond = cond; u.use_cond = use_cond ? 1 : 0;
-    // exactly RT CTAs: CTA c forms the FLAT order's strided sum of thread c
-    k_update<<<kUpdateCtas, RT, 0, h->s>>>(u);
+    // one resident wave: the loop role sums the operator's partials once per CTA
+    const long long wave = (long long)h->n_sm * kUpdateCtasPerSm;
+    k_update<<<(int)std::min<long long>(h->part.nflat, wave), RT, 0, h->s>>>(u);
 }
 
 void launch_reduce(hs_solver* h, int kind, const double* a, const double* b, double* out) {
@@ -459,8 +460,7 @@ hs_status hs_create(const hs_options* opt, const double* k_host, const double* r
     HS_CUDA(h->T.alloc(Nn)); HS_CUDA(h->b.alloc(Nn)); HS_CUDA(h->r.alloc(Nn)); HS_CUDA(h->z.alloc(Nn));
     HS_CUDA(h->p0.alloc(Nn)); HS_CUDA(h->p1.alloc(Nn)); HS_CUDA(h->Ap.alloc(Nn));
     HS_CUDA(h->partials.alloc((size_t)MAXQ * std::max(h->cp.ntiles, h->part.nflat) + 4096));
-    // the update's per-CTA strided sums: 3 quantities x RT CTAs
-    HS_CUDA(h->upart.alloc((size_t)3 * RT + 256));
+    HS_CUDA(h->upart.alloc((size_t)3 * h->part.nflat + 256));
     HS_CUDA(h->ticket.alloc(1)); HS_CUDA(h->st.alloc(1)); HS_CUDA(h->red.alloc(8)); HS_CUDA(h->sp.alloc(2));
     HS_CUDA(cudaMemsetAsync(h->ticket.p, 0, sizeof(unsigned), h->s));
     HS_CUDA(cudaMemsetAsync(h->st.p, 0, sizeof(DevState), h->s));
