@@ -93,10 +93,9 @@ typedef struct hs_step_record {
     double solve_ms;    /* build_rhs + PCG (+ reprojection) device time of the step */
 } hs_step_record;
 
-/* canonical reduction orders of an N-element grid: the operator's column
- * partition (cx planes per x-slab, ty node rows per lane, tz node columns per
- * full warp segment, rt threads = bpt warps per tile) and the flat order's
- * nodes per thread kf */
+/* canonical reduction orders of an N-element grid: the operator's slab tile
+ * (planes cx, rows ty, columns tz; rt threads of bpt positions each, halo
+ * included) and the flat order's nodes per thread kf */
 typedef struct hs_layout_info { int cx, ty, tz, rt, bpt, kf; } hs_layout_info;
 
 void        hs_default_options(hs_options* opt);
@@ -247,8 +246,8 @@ typedef struct hs_batch_options {
     int max_outer;        /* corrections per step */
     int max_inner;        /* inner PCG iterations per correction */
     int detect;           /* ABFT checksum on every operator apply */
-    int tile_planes;      /* operator x-slabs span min(N+1, tile_planes) planes; 0: a depth set by N
-                             alone (the single-instance choice when >= 16 planes, else 16) */
+    int tile_planes;      /* operator tiles span min(N+1, tile_planes) planes; 0: a depth set by N
+                             alone (the instance by itself fills the GPU, within 8..32 planes) */
     int device;
     int extrapolate;      /* start each step (after the first) from 2 T - T_prev instead of T */
 } hs_batch_options;

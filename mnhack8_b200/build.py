@@ -18,7 +18,7 @@ LIB = os.path.join(HERE, "libheat_b200.so")
 CLI = os.path.join(HERE, "heat_solver_b200")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = ["hs_solver.cu", "hs_setup.cpp", "hs_cli.cpp"]
-HEADERS = ["hs_kernels.cuh", "hs_types.h", "hs_host.h", "hs_cli.h", "hs_noalloc.cu", "hs_campaign.cu", "hs_batch.cu", "hs_batch_kernels.cuh", "hs_colop.cuh", "hs_csum.h", "hs_field.cu"]
+HEADERS = ["hs_kernels.cuh", "hs_types.h", "hs_host.h", "hs_cli.h", "hs_noalloc.cu", "hs_campaign.cu", "hs_batch.cu", "hs_batch_kernels.cuh", "hs_csum.h", "hs_field.cu"]
 
 
 def _nvcc() -> str:

@@ -4,9 +4,9 @@
 // independent solves (different N, dt, fields, step counts) live in slots of
 // one handle and advance together: hs_batch_step runs one implicit-Euler step
 // of every instance that has steps left, as one CUDA-graph launch:
-//   b = M T (FP64 column-march operator, ABFT checked);
+//   b = M T (FP64 slab operator, ABFT checked);
 //   start from T, or from 2 T - T_prev (extrapolate, from the second step);
-//   r = b - A T (FP64 column-march operator, ABFT checked), test ||r|| / ||b|| < rtol;
+//   r = b - A T (FP64 slab operator, ABFT checked), test ||r|| / ||b|| < rtol;
 //   while not converged (bounded by max_outer):
 //       FP32 Jacobi-PCG on A d = r to inner_tol (bounded by max_inner),
 //       every launch covering the tiles of all instances still iterating;
@@ -21,28 +21,43 @@
 
 namespace {
 
-// flat partition of one batched instance (vector work and its reductions)
-Part batch_part(int N) {
+// tile shape of one batched instance, a function of N and planes alone so that
+// an instance's arithmetic never depends on the rest of the batch.  planes == 0:
+// an instance large enough to fill the GPU by itself with tiles of at least 8
+// planes takes the single-instance slab layout (the FP64 operator's, whose
+// cost model counts waves over SLAB_SLOTS); a smaller one takes C, R with the
+// fewest positions loaded per node and the depth at which it would fill
+// SLAB_SLOTS tiles, within 8..32.  planes > 0: those C, R and min(N+1, planes).
+Part batch_part(int N, int planes) {
+    const long long NN = N + 1;
+    if (planes < 1 && slab_layout(N).CX >= 8) return make_part(N);
+    long long bestC = NN, bestR = 1, best_cost = -1;
+    const long long cmin = NN < 30 ? NN : 30;
+    for (long long C = cmin; C <= NN; ++C) {
+        const long long Cw = C + 2;
+        const long long Rmax = SPOS / Cw - 2;
+        if (Rmax < 1) break;
+        const long long R = Rmax < NN ? Rmax : NN;
+        const long long NCB = (NN + C - 1) / C, NRB = (NN + R - 1) / R;
+        const long long cost = NCB * NRB * (Cw * (R + 2) + 2 * (C + 1) * (R + 1));
+        if (best_cost < 0 || cost < best_cost) { best_cost = cost; bestC = C; bestR = R; }
+    }
+    const long long tyz = ((NN + bestC - 1) / bestC) * ((NN + bestR - 1) / bestR);
+    long long depth = planes;
+    if (planes < 1) {
+        depth = (NN * tyz + SLAB_SLOTS - 1) / SLAB_SLOTS;
+        depth = depth < 8 ? 8 : (depth > 32 ? 32 : depth);
+    }
+    const long long CX = depth < NN ? depth : NN;
     Part p{};
-    p.N = N; p.NN = N + 1;
-    p.Nn = (long long)p.NN * p.NN * p.NN;
+    p.N = N; p.NN = (int)NN;
+    p.C = (int)bestC; p.R = (int)bestR; p.CX = (int)CX;
+    p.Cw = p.C + 2; p.Rw = p.R + 2;
+    p.NCB = (int)((NN + bestC - 1) / bestC); p.NRB = (int)((NN + bestR - 1) / bestR); p.NXB = (int)((NN + CX - 1) / CX);
+    p.ntiles = (long long)p.NCB * p.NRB * p.NXB; p.nblk = p.ntiles;
+    p.Nn = NN * NN * NN;
     p.nflat = (p.Nn + (long long)RT * KF - 1) / ((long long)RT * KF);
     return p;
-}
-
-// Column partition of one batched instance (the FP64 solver's, hs_types.h),
-// with the x-slab depth: planes > 0, or else the single-instance choice when
-// it is at least 16 planes, else 16 (small instances share the GPU, so they
-// take deeper slabs than they would alone).  A function of N and planes only.
-ColLayout batch_col(int N, int planes) {
-    ColLayout L = col_layout(N);
-    int CX = planes > 0 ? planes : (L.CX >= 16 ? L.CX : 16);
-    if (CX > L.NN) CX = L.NN;
-    L.CX = CX;
-    L.NXB = (L.NN + CX - 1) / CX;
-    L.ntasks = (long long)L.NXB * L.TPS;
-    L.ntiles = (L.ntasks + CW - 1) / CW;
-    return L;
 }
 
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -60,8 +75,7 @@ struct hs_batch {
         int flip_step = -1, flip_bit = 0;   // armed level-G flip (T[flip_idx] before step flip_step)
         long long flip_idx = 0;
         hs_batch_fault fault{};             // armed vector fault (level 5/6/7, FP32 inner vectors)
-        Part part{};              // flat blocks
-        ColLayout col{};          // operator tiles
+        Part part{};
         void* mem = nullptr;      // one allocation holding every buffer of the instance
         BInst desc{};
         bool in_step = false;     // part of the step in flight
@@ -96,6 +110,18 @@ struct hs_batch {
 
 namespace {
 
+void set_bsmem() {
+    static bool done = false;
+    if (done) return;
+    done = true;
+    cudaFuncSetAttribute(kb_apply<double, BK_RESID>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(BSlabSmem<double>));
+    cudaFuncSetAttribute(kb_apply<double, BK_RHS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(BSlabSmem<double>));
+    cudaFuncSetAttribute(kb_apply<float, BK_LOOP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(BSlabSmem<float>));
+}
+
 BatchArgs batch_args(hs_batch* b) {
     BatchArgs a{};
     a.inst = b->d_inst.p; a.tile2inst = b->d_t2i.p; a.flat2inst = b->d_f2i.p;
@@ -113,7 +139,7 @@ BatchArgs batch_args(hs_batch* b) {
 // drop the graph) when they no longer fit; upload maps and descriptors
 hs_status upload(hs_batch* b) {
     long long nt = 0, nf = 0;
-    for (auto& sl : b->slots) if (sl.used) { nt += sl.col.ntiles; nf += sl.part.nflat; }
+    for (auto& sl : b->slots) if (sl.used) { nt += sl.part.ntiles; nf += sl.part.nflat; }
     if (nt > b->cap_tiles || nf > b->cap_flat || !b->d_t2i.p) {
         b->cap_tiles = std::max<long long>({nt, 2 * b->cap_tiles, 1024});
         b->cap_flat = std::max<long long>({nf, 2 * b->cap_flat, 1024});
@@ -134,9 +160,9 @@ hs_status upload(hs_batch* b) {
         d.active = 0;
         if (sl.used) {
             d.tile0 = t0; d.flat0 = f0;
-            for (long long t = 0; t < sl.col.ntiles; ++t) t2i[t0 + t] = (int)i;
+            for (long long t = 0; t < sl.part.ntiles; ++t) t2i[t0 + t] = (int)i;
             for (long long f = 0; f < sl.part.nflat; ++f) f2i[f0 + f] = (int)i;
-            t0 += sl.col.ntiles; f0 += sl.part.nflat;
+            t0 += sl.part.ntiles; f0 += sl.part.nflat;
             d.active = sl.steps_left > 0 ? 1 : 0;
         }
         sl.desc.tile0 = d.tile0; sl.desc.flat0 = d.flat0;
@@ -152,7 +178,7 @@ hs_status upload(hs_batch* b) {
 
 // outer-iteration tail: r = b - A T, test, start of the next inner solve
 void enqueue_resid(hs_batch* b, const BatchArgs& a) {
-    kb_apply<double, BK_RESID><<<(int)a.ntiles, RT, 0, b->s>>>(a);
+    kb_apply<double, BK_RESID><<<(int)a.ntiles, ST, sizeof(BSlabSmem<double>), b->s>>>(a);
     kb_final_apply<BK_RESID><<<a.n_inst, RT, 0, b->s>>>(a);
     kb_resid<<<(int)a.nflat, RT, 0, b->s>>>(a);
     kb_outer_final<<<a.n_inst, RT, 0, b->s>>>(a);
@@ -169,7 +195,7 @@ hs_status build_batch_graph(hs_batch* b) {
     cudaGraph_t pre;
     HS_CUDA(cudaStreamBeginCapture(b->s, cudaStreamCaptureModeThreadLocal));
     kb_step_begin<<<(a.n_inst + 127) / 128, 128, 0, b->s>>>(a);
-    kb_apply<double, BK_RHS><<<(int)a.ntiles, RT, 0, b->s>>>(a);
+    kb_apply<double, BK_RHS><<<(int)a.ntiles, ST, sizeof(BSlabSmem<double>), b->s>>>(a);
     kb_final_apply<BK_RHS><<<a.n_inst, RT, 0, b->s>>>(a);
     kb_extrapolate<<<(int)a.nflat, RT, 0, b->s>>>(a);
     enqueue_resid(b, a);
@@ -206,7 +232,7 @@ hs_status build_batch_graph(hs_batch* b) {
     HS_CUDA(cudaStreamBeginCaptureToGraph(b->s, ibody, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     // four inner iterations per pass (an instance that is done skips them), one condition
     for (int u = 0; u < 4; ++u) {
-        kb_apply<float, BK_LOOP><<<(int)a.ntiles, RT, 0, b->s>>>(a);
+        kb_apply<float, BK_LOOP><<<(int)a.ntiles, ST, sizeof(BSlabSmem<float>), b->s>>>(a);
         kb_final_apply<BK_LOOP><<<a.n_inst, RT, 0, b->s>>>(a);
         kb_update32<<<(int)a.nflat, RT, 0, b->s>>>(a);
         kb_final_update32<<<a.n_inst, RT, 0, b->s>>>(a);
@@ -242,7 +268,7 @@ hs_status step_direct(hs_batch* b) {
         return HS_OK;
     };
     kb_step_begin<<<(a.n_inst + 127) / 128, 128, 0, b->s>>>(a);
-    kb_apply<double, BK_RHS><<<(int)a.ntiles, RT, 0, b->s>>>(a);
+    kb_apply<double, BK_RHS><<<(int)a.ntiles, ST, sizeof(BSlabSmem<double>), b->s>>>(a);
     kb_final_apply<BK_RHS><<<a.n_inst, RT, 0, b->s>>>(a);
     kb_extrapolate<<<(int)a.nflat, RT, 0, b->s>>>(a);
     enqueue_resid(b, a);
@@ -254,7 +280,7 @@ hs_status step_direct(hs_batch* b) {
         for (;;) {
             if (read(1) != HS_OK) return HS_ERR_CUDA;
             if (!host_flag) break;
-            kb_apply<float, BK_LOOP><<<(int)a.ntiles, RT, 0, b->s>>>(a);
+            kb_apply<float, BK_LOOP><<<(int)a.ntiles, ST, sizeof(BSlabSmem<float>), b->s>>>(a);
             kb_final_apply<BK_LOOP><<<a.n_inst, RT, 0, b->s>>>(a);
             kb_update32<<<(int)a.nflat, RT, 0, b->s>>>(a);
             kb_final_update32<<<a.n_inst, RT, 0, b->s>>>(a);
@@ -304,6 +330,7 @@ hs_status hs_batch_create(const hs_batch_options* opt, hs_batch** out) {
     HS_CUDA(cudaMemPoolSetAttribute(b->pool, cudaMemPoolAttrReleaseThreshold, &keep));
     int no = 0;                     // an add never waits on the step stream for a freed arena
     HS_CUDA(cudaMemPoolSetAttribute(b->pool, cudaMemPoolReuseAllowInternalDependencies, &no));
+    set_bsmem();
     *out = b.release();
     return HS_OK;
 }
@@ -421,10 +448,8 @@ hs_status batch_add_impl(hs_batch* b, int N, double dt, const double* k, const d
     // the caller's host arrays are free again once this returns
     HS_CUDA(cudaStreamSynchronize(sa));
     sl.used = true; sl.N = N; sl.dt = dt; sl.steps_left = n_steps; sl.steps_done = 0;
-    sl.part = batch_part(N);
-    sl.col = batch_col(N, b->opt.tile_planes);
+    sl.part = batch_part(N, b->opt.tile_planes);
     d.part = sl.part;
-    d.col = sl.col;
     sl.mem = mem;
     sl.desc = d;
     b->dirty = true;
@@ -580,7 +605,7 @@ hs_status hs_batch_info(hs_batch* b, int slot, hs_batch_inst_info* out) {
     out->inner_iters = st.inner_total; out->outer_iters = st.outer_total;
     out->applies32 = st.applies32; out->applies64 = st.applies64;
     out->rel_residual = st.rel64; out->d1_max64 = st.d1_max64; out->d1_max32 = st.d1_max32;
-    out->tiles = sl.col.ntiles;
+    out->tiles = sl.part.ntiles;
     out->fault_fired = st.fi_fired; out->stalls = st.stalls; out->inner_faults = st.inner_faults;
     return HS_OK;
 }

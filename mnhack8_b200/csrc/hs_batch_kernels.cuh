@@ -1,9 +1,9 @@
 // hs_batch_kernels.cuh -- kernels of the batched mixed-precision solver
 // (hs_batch.cu).  Many independent transient-heat solves advance together:
-// every launch covers the operator tiles (column partition) or flat blocks (vector work)
+// every launch covers the slab tiles (operator) or flat blocks (vector work)
 // of all instances, and a block finds its instance through a map.  Each
 // implicit-Euler step solves (M + dt K) T = M T_old by defect correction:
-// FP64 residual r = b - A T (the column-march operator in FP64, ABFT checked),
+// FP64 residual r = b - A T (the slab operator in FP64, ABFT checked),
 // an FP32 Jacobi-PCG solve of A d = r to a loose relative tolerance (FP32
 // operator and preconditioner, FP64 dot products of the FP32 values), and
 // T += d in FP64, until ||b - A T|| / ||b|| < rtol.
@@ -92,8 +92,7 @@ __device__ __forceinline__ bool fi_now(const BState* st, int vec) {
 
 // instance descriptor (device array, rewritten by the host between rounds)
 struct BInst {
-    Part part;                 // flat blocks of this instance (vector work)
-    ColLayout col;             // operator tiles of this instance (column partition)
+    Part part;                 // slab tiles and flat blocks of this instance
     long long tile0, flat0;    // first global tile / flat block
     double dt;
     double cm[4], ck[4];       // wht eigen-constants / 8 of this grid
@@ -171,34 +170,38 @@ __device__ __forceinline__ void elem_wht_v(V* v, V rhoc, V dk, const V* cm, cons
             if (!(q & bit)) { const V u = v[q], w = v[q | bit]; v[q] = T::add(u, w); v[q | bit] = T::sub(u, w); }
 }
 
-// Batched operator, column-march warps (the FP64 solver's k_apply_col design,
-// hs_colop.cuh) in precision V on one instance's column partition.  KIND 0:
-// y64 = A T (FP64, residual); 1: b = M T (FP64, right-hand side); 2: inner
-// FP32 loop, p = z (+ beta p), Ap = A p.  Partials per tile, compensated
-// (hi, lo): p.Ap (KIND 2) and D1: 1_int.y, w.x, x.x.
-enum BKind { BK_RESID = 0, BK_RHS = 1, BK_LOOP = 2 };
-
 template <typename V>
-struct BColStep {
-    V a0, a1, b0, b1, cr, ck;
-    double w;
+struct __align__(16) BSlabSmem {
+    V P[2][SPOS];
+    typename VTraits<V>::V2 Y1[SPOS], Y2[SPOS], Y3[SPOS];
+    double sh[2 * MAXQ][8];
 };
 
-__device__ __forceinline__ float flipv(float x, int bit) { return flipf(x, bit); }
-__device__ __forceinline__ double flipv(double x, int bit) { return flipbit(x, bit); }
+// Batched slab operator.  KIND 0: y64 = A T (FP64, residual); 1: b = M T
+// (FP64, right-hand side); 2: inner FP32 loop, p = z (+ beta p), Ap = A p.
+// Partials per tile: p.Ap (KIND 2), and D1: 1_int.y, w.x, x.x.
+enum BKind { BK_RESID = 0, BK_RHS = 1, BK_LOOP = 2 };
 
-// FI false: no vector fault is armed for this launch
+// tile t of instance I; FI false: no vector fault is armed for this launch
 template <typename V, int KIND, bool FI>
-__device__ __forceinline__ void kb_col_march(const BatchArgs& B, const BInst& I, const ColLane& C,
-                                             CSum (&part)[MAXQ]) {
+__device__ __forceinline__ void kb_tile(const BatchArgs& B, BSlabSmem<V>& S, long long t, const BInst& I) {
+    using T2 = typename VTraits<V>::V2;
     using VT = VTraits<V>;
-    using V2 = typename VT::V2;
-    constexpr int NS = CR + 2;
-    static_assert(NS % 3 == 0, "three rotating load sets per layer");
     BState* st = I.st;
     const bool loop = KIND == BK_LOOP;
-    const int N = I.col.N, NN = I.col.NN;
-    const int ec = C.ec, r0 = C.r0, xa = C.xa, xb = C.xb;
+    if constexpr (KIND == BK_LOOP) {
+        if (st->odone || st->done) return;
+    } else if constexpr (KIND == BK_RESID) {
+        if (st->odone) return;
+    }
+    const Part& P = I.part;
+    const int N = P.N, Cw = P.Cw;
+    // node and element indices fit in 32 bits (N <= 1200)
+    const unsigned plane = (unsigned)P.NN * (unsigned)P.NN, eplane = (unsigned)N * (unsigned)N;
+    const SlabTile Tt = slab_tile(P, t - I.tile0);
+    const SlabPos G = slab_pos(P, Tt, threadIdx.x);
+    const unsigned fl = G.fl;
+    const int tid = threadIdx.x, xa = Tt.xa, xb = Tt.xb;
     const V dtv = (V)((KIND == BK_RHS) ? 0.0 : I.dt);
     V cm[4], ck[4];
 #pragma unroll
@@ -206,212 +209,177 @@ __device__ __forceinline__ void kb_col_march(const BatchArgs& B, const BInst& I,
         cm[j] = (sizeof(V) == 4) ? (V)I.cmf[j] : (V)I.cm[j];
         ck[j] = (sizeof(V) == 4) ? (V)I.ckf[j] : (V)I.ck[j];
     }
+    // inputs
     const int iter = loop ? st->iter : 0;
-    const V beta = (V)(loop ? st->beta : 0.0);
-    const V* srcA;
-    const V* srcB = nullptr;
+    const double betad = loop ? st->beta : 0.0;
+    const V beta = (V)betad;
+    const V* src_a;
+    const V* src_b = nullptr;
     V* pout = nullptr;
     V* yout;
     if constexpr (KIND == BK_LOOP) {
-        srcA = reinterpret_cast<const V*>(I.z32);
-        srcB = (iter > 0) ? reinterpret_cast<const V*>((iter & 1) ? I.p32a : I.p32b) : nullptr;
+        src_a = reinterpret_cast<const V*>(I.z32);
+        src_b = (iter > 0) ? reinterpret_cast<const V*>((iter & 1) ? I.p32a : I.p32b) : nullptr;
         pout = reinterpret_cast<V*>((iter & 1) ? I.p32b : I.p32a);
         yout = reinterpret_cast<V*>(I.Ap32);
     } else {
-        srcA = reinterpret_cast<const V*>(I.T);
+        src_a = reinterpret_cast<const V*>(I.T);
         yout = reinterpret_cast<V*>(KIND == BK_RHS ? I.b : I.y64);
     }
-    const bool two = srcB != nullptr;
+    const bool two = src_b != nullptr;
     const double* w = (KIND == BK_RHS) ? I.wM : I.wA;
     const bool d1 = B.detect != 0;
+    CSum part[MAXQ] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+
+    V pA[SK], pB[SK], aA[SK], aB[SK], ra[SK], rb[SK], cr[SK], ckk[SK];
+    double wv[SK];
+    auto ld_raw = [&](int px) {
+        const bool pv = px >= 0 && px <= N;
+        const unsigned base = (unsigned)px * plane;
+#pragma unroll
+        for (int k = 0; k < SK; ++k) {
+            const bool v = pv && sp_valid(fl, k);
+            const unsigned n = base + (unsigned)G.noff[k];
+            ra[k] = v ? __ldg(src_a + n) : (V)0;
+            rb[k] = (v && two) ? __ldg(src_b + n) : (V)0;
+        }
+    };
     int fi_p = 0, fi_ap = 0, fi_bit = 0;
     long long fi_idx = -1;
     if constexpr (KIND == BK_LOOP && FI) {
         fi_p = fi_now(st, FI_P); fi_ap = fi_now(st, FI_AP);
         fi_bit = st->fi_bit; fi_idx = st->fi_idx;
     }
-    const bool live = C.fl & 1u;
-    const bool own = (C.fl & 2u) && ec <= N;
-    const bool colv = live && ec >= 0 && ec <= N;
-    const bool colv1 = live && ec + 1 >= 0 && ec + 1 <= N;
-    const bool ecv = live && ec >= 0 && ec < N;
-    unsigned rowv = 0u, erowv = 0u, orow = 0u;
+    auto form = [&](V (&p)[SK], int px) {
 #pragma unroll
-    for (int i = 0; i < NS; ++i) {
-        const int r = r0 - 1 + i;
-        if (r >= 0 && r <= N) rowv |= 1u << i;
-        if (i >= 1 && r - 1 >= 0 && r - 1 < N) erowv |= 1u << i;
-        if (own && i >= 1 && i <= CR && r <= N) orow |= 1u << i;
-    }
-    if (own && (C.fl & 4u)) orow |= 1u << (NS - 1);
-    const int lane_n = (r0 - 1) * NN + ec;
-    const int lane_e = (r0 - 2) * N + ec;
-
-    auto load = [&](BColStep<V>& S, int x, int i) {
-        const int xp = x + 1;
-        const bool pv = xp >= 0 && xp <= N && xp <= xb + 1 && ((rowv >> i) & 1u);
-        const int n = xp * NN * NN + lane_n + i * NN;
-        const bool v0 = pv && colv, v1 = pv && colv1;
-        S.a0 = v0 ? __ldg(srcA + n) : (V)0;
-        S.a1 = v1 ? __ldg(srcA + n + 1) : (V)0;
-        S.b0 = (v0 && two) ? __ldg(srcB + n) : (V)0;
-        S.b1 = (v1 && two) ? __ldg(srcB + n + 1) : (V)0;
-        S.w = (d1 && v0 && xp >= xa && xp <= xb && ((orow >> i) & 1u)) ? __ldg(w + n) : 0.0;
-        const bool ev = i >= 1 && x >= xa - 1 && x >= 0 && x < N && ecv && ((erowv >> i) & 1u);
-        const int e = x * N * N + lane_e + i * N;
-        if constexpr (sizeof(V) == 4) {
-            const float2 c = ev ? __ldg(I.coef32 + e) : make_float2(0.f, 0.f);
-            S.cr = c.x; S.ck = c.y;
-        } else {
-            const double2 c = ev ? __ldg(I.coef64 + e) : make_double2(0.0, 0.0);
-            S.cr = c.x; S.ck = c.y;
+        for (int k = 0; k < SK; ++k) p[k] = two ? VT::fma(beta, rb[k], ra[k]) : ra[k];
+        if constexpr (KIND == BK_LOOP && FI) {
+            if (fi_p) {
+#pragma unroll
+                for (int k = 0; k < SK; ++k)
+                    if (sp_valid(fl, k) && (long long)px * plane + G.noff[k] == fi_idx) {
+                        p[k] = flipf(p[k], fi_bit);
+                        st->fi_fired = 1;
+                    }
+            }
         }
     };
-
-    V fp[CR + 1][4];
-    V slo[CR + 1];
-    V pk[CR + 1];
+    auto ld_coef = [&](int ex) {
+        const bool ev = ex >= 0 && ex < N;
+        const unsigned base = (unsigned)ex * eplane;
 #pragma unroll
-    for (int j = 0; j <= CR; ++j) {
-        slo[j] = (V)0; pk[j] = (V)0;
-        fp[j][0] = fp[j][1] = fp[j][2] = fp[j][3] = (V)0;
-    }
-    BColStep<V> B0, B1, B2;
-    load(B0, xa - 2, 0);
-    load(B1, xa - 2, 1);
-    for (int x = xa - 2; x <= xb; ++x) {
-        const bool el = x >= xa - 1 && x >= 0 && x < N;
-        const bool cpl = x >= xa;
-        const bool fown = x + 1 >= xa && x + 1 <= xb;
-        V zsP_s = (V)0, zsP_d = (V)0, pnA = (V)0;
-        V hq2 = (V)0, hL3 = (V)0, hq6 = (V)0, hL7 = (V)0;
+        for (int k = 0; k < SK; ++k) {
+            const bool v = ev && sp_elem(fl, k);
+            const unsigned e = base + (unsigned)G.eoff[k];
+            if constexpr (sizeof(V) == 4) {
+                const float2 c = v ? __ldg(I.coef32 + e) : make_float2(0.f, 0.f);
+                cr[k] = c.x; ckk[k] = c.y;
+            } else {
+                const double2 c = v ? __ldg(I.coef64 + e) : make_double2(0.0, 0.0);
+                cr[k] = c.x; ckk[k] = c.y;
+            }
+        }
+    };
+    auto ld_w = [&](int px) {
+        const bool pv = px >= xa && px <= xb;
+        const unsigned base = (unsigned)px * plane;
 #pragma unroll
-        for (int i = 0; i < NS; ++i) {
-            BColStep<V>& S = (i % 3 == 0) ? B0 : (i % 3 == 1) ? B1 : B2;
-            const V a0 = S.a0, a1 = S.a1, b0 = S.b0, b1 = S.b1, cr = S.cr, ckk = S.ck;
-            const double wv = S.w;
-            {
-                BColStep<V>& SL = ((i + 2) % 3 == 0) ? B0 : ((i + 2) % 3 == 1) ? B1 : B2;
-                if (i + 2 < NS) load(SL, x, i + 2);
-                else load(SL, x + 1, i + 2 - NS);
-            }
-            const int r = r0 - 1 + i;
-            V pA = two ? VT::fma(beta, b0, a0) : a0;
-            V pB = two ? VT::fma(beta, b1, a1) : a1;
-            const int nrow = (x + 1) * NN * NN + lane_n + i * NN;
-            if constexpr (KIND == BK_LOOP && FI) {
-                if (fi_p && x + 1 <= N && ((rowv >> i) & 1u)) {
-                    if (colv && (long long)nrow == fi_idx) { pA = flipv(pA, fi_bit); st->fi_fired = 1; }
-                    if (colv1 && (long long)nrow + 1 == fi_idx) { pB = flipv(pB, fi_bit); st->fi_fired = 1; }
-                }
-            }
-            if (fown && ((orow >> i) & 1u)) {
-                if (loop) __stwb(pout + nrow, pA);
-                if (d1) {
-                    const double pd = (double)pA;
-                    csum_fma(part[2], wv, pd);
-                    part[3].hi = dfma(pd, pd, part[3].hi);     // the norm only scales the threshold
-                }
-            }
-            const V zs_s = VT::add(pA, pB), zs_d = VT::sub(pA, pB);
-            if (i >= 1) {
-                const int j = i - 1;
+        for (int k = 0; k < SK; ++k)
+            wv[k] = (pv && d1 && sp_out(fl, k)) ? __ldg(w + (base + (unsigned)G.noff[k])) : 0.0;
+    };
+    auto layer = [&](int ix, int cur, V (&pc)[SK], V (&pn)[SK], V (&ac)[SK], V (&an)[SK]) {
+        const int nxt = cur ^ 1;
+        form(pn, ix + 1);
+#pragma unroll
+        for (int k = 0; k < SK; ++k) S.P[nxt][tid + k * ST] = pn[k];
+        ld_raw(ix + 2 <= xb + 1 ? ix + 2 : -2);
+        __syncthreads();
+        if (ix >= 0 && ix < N) {
+#pragma unroll
+            for (int k = 0; k < SK; ++k) {
+                if (!sp_elem(fl, k)) continue;
+                const int j = tid + k * ST;
                 V v[8];
-                const V f0 = VT::add(zsP_s, zs_s), f1 = VT::add(zsP_d, zs_d);
-                const V f2 = VT::sub(zsP_s, zs_s), f3 = VT::sub(zsP_d, zs_d);
-                if (el) {
-                    v[0] = VT::add(fp[j][0], f0); v[1] = VT::add(fp[j][1], f1);
-                    v[2] = VT::add(fp[j][2], f2); v[3] = VT::add(fp[j][3], f3);
-                    v[4] = VT::sub(fp[j][0], f0); v[5] = VT::sub(fp[j][1], f1);
-                    v[6] = VT::sub(fp[j][2], f2); v[7] = VT::sub(fp[j][3], f3);
-                    const V dk = VT::mul(dtv, ckk);
-                    const V l0 = VT::mul(cr, cm[0]);
-                    const V l1 = VT::fma(dk, ck[1], VT::mul(cr, cm[1]));
-                    const V l2 = VT::fma(dk, ck[2], VT::mul(cr, cm[2]));
-                    const V l3 = VT::fma(dk, ck[3], VT::mul(cr, cm[3]));
-                    v[0] = VT::mul(v[0], l0);
-                    v[1] = VT::mul(v[1], l1); v[2] = VT::mul(v[2], l1); v[4] = VT::mul(v[4], l1);
-                    v[3] = VT::mul(v[3], l2); v[5] = VT::mul(v[5], l2); v[6] = VT::mul(v[6], l2);
-                    v[7] = VT::mul(v[7], l3);
-#pragma unroll
-                    for (int bit = 1; bit <= 4; bit <<= 1)
-#pragma unroll
-                        for (int q = 0; q < 8; ++q)
-                            if (!(q & bit)) { const V u = v[q], t = v[q | bit]; v[q] = VT::add(u, t); v[q | bit] = VT::sub(u, t); }
-                } else {
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) v[q] = (V)0;
-                }
-                fp[j][0] = f0; fp[j][1] = f1; fp[j][2] = f2; fp[j][3] = f3;
-                const V L1 = __shfl_up_sync(0xffffffffu, v[1], 1), L3 = __shfl_up_sync(0xffffffffu, v[3], 1);
-                const V L5 = __shfl_up_sync(0xffffffffu, v[5], 1), L7 = __shfl_up_sync(0xffffffffu, v[7], 1);
-                if (j >= 1) {
-                    const int oj = j - 1;
-                    if (cpl && ((orow >> j) & 1u)) {
-                        const int er = r - 1;
-                        const int n = x * NN * NN + lane_n + j * NN;
-                        const bool bnd = x == 0 || x == N || er == 0 || er == N || ec == 0 || ec == N;
-                        V y = bnd ? (V)0 : VT::add(VT::add(VT::add(VT::add(slo[oj], v[0]), hL3), hq2), L1);
-                        if constexpr (KIND == BK_LOOP && FI) {
-                            if (fi_ap && (long long)n == fi_idx) { y = flipv(y, fi_bit); st->fi_fired = 1; }
-                        }
-                        const double yd = (double)y;
-                        if (loop) csum_fma(part[0], (double)pk[oj], yd);
-                        if (d1 && !bnd) csum_add(part[1], yd);
-                        __stwb(yout + n, y);
-                    }
-                    slo[oj] = VT::add(VT::add(VT::add(VT::add((V)0, v[4]), hL7), hq6), L5);
-                    pk[oj] = pnA;
-                }
-                hq2 = v[2]; hL3 = L3; hq6 = v[6]; hL7 = L7;
+                v[0] = pc[k];
+                v[1] = S.P[cur][j + 1];
+                v[2] = S.P[cur][j + Cw];
+                v[3] = S.P[cur][j + Cw + 1];
+                v[4] = pn[k];
+                v[5] = S.P[nxt][j + 1];
+                v[6] = S.P[nxt][j + Cw];
+                v[7] = S.P[nxt][j + Cw + 1];
+                elem_wht_v<V>(v, cr[k], VT::mul(dtv, ckk[k]), cm, ck);
+                ac[k] = VT::add(ac[k], v[0]);
+                an[k] = VT::add((V)0, v[4]);
+                S.Y1[j + 1] = T2{v[1], v[5]};
+                S.Y2[j + Cw] = T2{v[2], v[6]};
+                S.Y3[j + Cw + 1] = T2{v[3], v[7]};
             }
-            zsP_s = zs_s; zsP_d = zs_d;
-            pnA = pA;
         }
-        if (C.fl & 4u) {
-            if (cpl && own) {
-                const int n = (x * NN + N) * NN + ec;
-                V y = (V)0;
+        ld_coef(ix + 1 <= xb ? ix + 1 : -1);
+        __syncthreads();
+        const unsigned base = (unsigned)ix * plane;
+        const bool xbnd = ix == 0 || ix == N;
+#pragma unroll
+        for (int k = 0; k < SK; ++k) {
+            if (!sp_out(fl, k)) continue;
+            const int j = tid + k * ST;
+            const bool yzin = !sp_yzb(fl, k);
+            T2 y3{(V)0, (V)0}, y2 = y3, y1 = y3;
+            if (yzin) { y3 = S.Y3[j]; y2 = S.Y2[j]; y1 = S.Y1[j]; }
+            if (ix >= xa) {
+                const unsigned n = base + (unsigned)G.noff[k];
+                const bool bnd = !yzin || xbnd;
+                V y = bnd ? (V)0 : VT::add(VT::add(VT::add(ac[k], y3.x), y2.x), y1.x);
                 if constexpr (KIND == BK_LOOP && FI) {
-                    if (fi_ap && (long long)n == fi_idx) { y = flipv(y, fi_bit); st->fi_fired = 1; }
+                    if (fi_ap && (long long)n == fi_idx) { y = flipf(y, fi_bit); st->fi_fired = 1; }
                 }
-                if (loop) csum_fma(part[0], (double)pk[CR], (double)y);
-                __stwb(yout + n, y);
+                const double pv = (double)pc[k], yd = (double)y;
+                if (loop) csum_fma(part[0], pv, yd);
+                if (d1) {
+                    if (!bnd) csum_add(part[1], yd);
+                    csum_fma(part[2], wv[k], pv);
+                    part[3].hi = dfma(pv, pv, part[3].hi);      // the norm only scales the threshold
+                }
+                __stwb(yout + n, y);                      // global stores (the pointers come from global memory)
+                if (loop) __stwb(pout + n, pc[k]);
             }
-            pk[CR] = pnA;
+            an[k] = yzin ? VT::add(VT::add(VT::add(an[k], y3.y), y2.y), y1.y) : (V)0;
         }
+        ld_w(ix + 1);
+    };
+    ld_raw(xa - 1);
+    form(pA, xa - 1);
+#pragma unroll
+    for (int k = 0; k < SK; ++k) { S.P[0][tid + k * ST] = pA[k]; aA[k] = (V)0; aB[k] = (V)0; }
+    ld_raw(xa);
+    ld_coef(xa - 1);
+    for (int ix = xa - 1; ix <= xb; ++ix) {
+        layer(ix, (ix - xa + 1) & 1, pA, pB, aA, aB);
+#pragma unroll
+        for (int k = 0; k < SK; ++k) { pA[k] = pB[k]; aA[k] = aB[k]; }
     }
+    if (!loop && !d1) return;
+    cta_tree_csum<MAXQ>(part, S.sh);
+    if (threadIdx.x == 0) store_cpartials<MAXQ>(part, B.pa, B.ntiles, t);
 }
 
 template <typename V, int KIND>
-__global__ void __launch_bounds__(RT, 1) kb_apply(BatchArgs B) {
-    __shared__ double sh[2 * MAXQ][8];
+__global__ void __launch_bounds__(ST, 2) kb_apply(BatchArgs B) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    BSlabSmem<V>& S = *reinterpret_cast<BSlabSmem<V>*>(smem_raw);
     const long long t = blockIdx.x;
     if (t >= B.ntiles) return;
     const int slot = B.tile2inst[t];
     if (slot < 0) return;
     const BInst& I = B.inst[slot];
     if (!I.active) return;
-    const BState* st = I.st;
     if constexpr (KIND == BK_LOOP) {
-        if (st->odone || st->done) return;
-    } else if constexpr (KIND == BK_RESID) {
-        if (st->odone) return;
+        if (fi_now(I.st, FI_P) || fi_now(I.st, FI_AP)) kb_tile<V, KIND, true>(B, S, t, I);
+        else kb_tile<V, KIND, false>(B, S, t, I);
+    } else {
+        kb_tile<V, KIND, false>(B, S, t, I);
     }
-    CSum part[MAXQ] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
-    const long long wt = (t - I.tile0) * CW + (threadIdx.x >> 5);
-    const ColLane C = col_lane(I.col, wt, threadIdx.x & 31);
-    if (wt < I.col.ntasks) {                       // warp-uniform
-        if constexpr (KIND == BK_LOOP) {
-            if (fi_now(st, FI_P) || fi_now(st, FI_AP)) kb_col_march<V, KIND, true>(B, I, C, part);
-            else kb_col_march<V, KIND, false>(B, I, C, part);
-        } else {
-            kb_col_march<V, KIND, false>(B, I, C, part);
-        }
-    }
-    if (KIND != BK_LOOP && !B.detect) return;
-    cta_tree_csum<MAXQ>(part, sh);
-    if (threadIdx.x == 0) store_cpartials<MAXQ>(part, B.pa, B.ntiles, t);
 }
 
 // compensated sums of one instance's partials: count (hi, lo) pairs per
@@ -464,7 +432,7 @@ __global__ void __launch_bounds__(RT) kb_final_apply(BatchArgs B) {
     if (KIND == BK_LOOP && (st->odone || st->done)) return;
     if (KIND == BK_RESID && st->odone) return;
     double p[MAXQ];
-    inst_sums<MAXQ>(p, B.pa + I.tile0, I.col.ntiles, B.ntiles, sh);
+    inst_sums<MAXQ>(p, B.pa + I.tile0, I.part.ntiles, B.ntiles, sh);
     if (threadIdx.x != 0) return;
     if (B.detect) {
         const double rel = d1_rel(p, KIND == BK_RHS ? st->norm_wM : st->norm_wA);

@@ -284,7 +284,7 @@ __device__ __forceinline__ void final_sums(double (&v)[NQ], const double* partia
 
 // ---- operator application: colored (deterministic gather) --------------------
 struct ApplyArgs {
-    ColLayout cp;
+    Part part;
     int N, role, form_pad;
     double dt_eff;
     const double* x;        // input (roles other than LOOP)
@@ -303,7 +303,215 @@ struct ApplyArgs {
     ElemConsts ec;
 };
 
-#include "hs_colop.cuh"
+// ---- colored operator: slab tiles ------------------------------------------------
+// One CTA of ST threads streams a tile's node planes in increasing x.  Per
+// element layer ix (between planes ix and ix+1):
+//   1. plane ix+1 is formed (p = z + beta p_{k-1} in the PCG loop) from
+//      registers loaded one layer ahead, kept in registers and published to
+//      shared memory;
+//   2. the element whose lower corner is a position (own column) gathers its
+//      six other corners from the two published planes, applies the element
+//      operator, folds its own-column outputs (q = 0 into the plane-ix node,
+//      q = 4 into the plane-(ix+1) node) into per-position accumulators and
+//      hands the other six to the three neighbouring positions;
+//   3. each tile node of plane ix adds the three handed-in contributions
+//      (q = 3, 2, 1), which completes its canonical node sum, and is
+//      projected, checked and stored; the plane-(ix+1) accumulators take
+//      q = 7, 6, 5.
+// Per node and layer that is one shared store of p, six shared loads for the
+// gather and three 16-byte stores and loads for the hand-over.
+struct __align__(16) SlabSmem {
+    double P[2][SPOS];      // formed planes, plane px in P[px & 1]
+    double2 Y1[SPOS];       // from the element at position j-1:      (q1, q5)
+    double2 Y2[SPOS];       // from the element at position j-Cw:     (q2, q6)
+    double2 Y3[SPOS];       // from the element at position j-Cw-1:   (q3, q7)
+    double sh[MAXQ][8];
+};
+constexpr size_t kSlabSmem = sizeof(SlabSmem);
+
+// MODE 0: input x as given; 1: PCG loop, p = z; 2: PCG loop, p = z + beta p_{k-1}.
+// FI false: no fault is armed for this launch (the per-node fault tests compile out).
+template <int FORM, int MODE, bool FI = true>
+__device__ __forceinline__ void slab_march(const ApplyArgs& a, SlabSmem& S, const SlabTile& T, const SlabPos& G,
+                                           const double* src_a, const double* src_b, double beta, double* pout,
+                                           bool loop, bool d1, bool rhs, int fi_p, int fi_ap, int fi_r, int fi_bit,
+                                           long long fi_idx, long long fi_elem, double (&part)[MAXQ]) {
+    constexpr bool TWO = MODE == 2;
+    if (!FI) { fi_p = 0; fi_ap = 0; fi_r = 0; }
+    const Part& P = a.part;
+    const int N = P.N, Cw = P.Cw;
+    // node and element indices fit in 32 bits (N <= 1200): one wide multiply-add per address
+    const unsigned plane = (unsigned)P.NN * (unsigned)P.NN, eplane = (unsigned)N * (unsigned)N;
+    const int tid = threadIdx.x;
+    const unsigned fl = G.fl;
+    const int xa = T.xa, xb = T.xb;
+
+    double pA[SK], pB[SK], aA[SK], aB[SK], ra[SK], rb[SK], cr[SK], ck[SK], wv[SK], fv[SK];
+    auto ld_raw = [&](int px) {
+        const bool pv = px >= 0 && px <= N;
+        const unsigned base = (unsigned)px * plane;
+#pragma unroll
+        for (int k = 0; k < SK; ++k) {
+            const bool v = pv && sp_valid(fl, k);
+            const unsigned n = base + (unsigned)G.noff[k];
+            ra[k] = v ? __ldg(src_a + n) : 0.0;
+            if (TWO) rb[k] = v ? __ldg(src_b + n) : 0.0;
+        }
+    };
+    auto form = [&](int px, double (&p)[SK]) {
+#pragma unroll
+        for (int k = 0; k < SK; ++k) {
+            double v = TWO ? dfma(beta, rb[k], ra[k]) : ra[k];
+            if (fi_p && sp_valid(fl, k) && (long long)px * plane + G.noff[k] == fi_idx) v = flipbit(v, fi_bit);
+            p[k] = v;
+        }
+    };
+    auto ld_coef = [&](int ex) {
+        const bool ev = ex >= 0 && ex < N;
+        const unsigned base = (unsigned)ex * eplane;
+#pragma unroll
+        for (int k = 0; k < SK; ++k) {
+            const bool v = ev && sp_elem(fl, k);
+            const double2 c = v ? __ldg(a.coef + (base + (unsigned)G.eoff[k])) : make_double2(0.0, 0.0);
+            cr[k] = c.x; ck[k] = c.y;
+        }
+    };
+    auto ld_w = [&](int px) {
+        const bool pv = px >= xa && px <= xb;
+        const unsigned base = (unsigned)px * plane;
+#pragma unroll
+        for (int k = 0; k < SK; ++k) {
+            const bool v = pv && sp_out(fl, k);
+            const unsigned n = base + (unsigned)G.noff[k];
+            wv[k] = (v && d1) ? __ldg(a.w + n) : 0.0;
+            if (MODE == 0) fv[k] = (v && rhs) ? __ldg(a.F + n) : 0.0;
+        }
+    };
+
+    // One element layer ix (between planes ix and ix+1).  Plane px lives in
+    // P[(px - xa + 1) & 1] (cur for plane ix); pc / pn hold planes ix / ix+1
+    // of the own column, ac / an the node sums of planes ix / ix+1.
+    auto layer = [&](int ix, int cur, double (&pc)[SK], double (&pn)[SK], double (&ac)[SK], double (&an)[SK]) {
+        const int nxt = cur ^ 1;
+        // 1. plane ix+1
+        form(ix + 1, pn);
+#pragma unroll
+        for (int k = 0; k < SK; ++k) S.P[nxt][tid + k * ST] = pn[k];
+        ld_raw(ix + 2 <= xb + 1 ? ix + 2 : -2);
+        __syncthreads();
+        // 2. element layer ix
+        if (ix >= 0 && ix < N) {
+#pragma unroll
+            for (int k = 0; k < SK; ++k) {
+                if (!sp_elem(fl, k)) continue;
+                const int j = tid + k * ST;
+                double v[8];
+                v[0] = pc[k];
+                v[1] = S.P[cur][j + 1];
+                v[2] = S.P[cur][j + Cw];
+                v[3] = S.P[cur][j + Cw + 1];
+                v[4] = pn[k];
+                v[5] = S.P[nxt][j + 1];
+                v[6] = S.P[nxt][j + Cw];
+                v[7] = S.P[nxt][j + Cw + 1];
+                elem_apply<FORM>(v, cr[k], ck[k], a.dt_eff, a.ec);
+                if (fi_r && (long long)ix * eplane + G.eoff[k] == fi_elem) v[0] = flipbit(v[0], fi_bit);
+                ac[k] = dadd(ac[k], v[0]);
+                an[k] = dadd(0.0, v[4]);
+                S.Y1[j + 1] = make_double2(v[1], v[5]);
+                S.Y2[j + Cw] = make_double2(v[2], v[6]);
+                S.Y3[j + Cw + 1] = make_double2(v[3], v[7]);
+            }
+        }
+        ld_coef(ix + 1 <= xb ? ix + 1 : -1);
+        __syncthreads();
+        // 3. tile nodes of plane ix; node sums of plane ix+1
+        const unsigned base = (unsigned)ix * plane;
+        const bool xbnd = ix == 0 || ix == N;
+#pragma unroll
+        for (int k = 0; k < SK; ++k) {
+            if (!sp_out(fl, k)) continue;
+            const int j = tid + k * ST;
+            const bool yzin = !sp_yzb(fl, k);
+            double2 y3 = make_double2(0.0, 0.0), y2 = y3, y1 = y3;
+            if (yzin) { y3 = S.Y3[j]; y2 = S.Y2[j]; y1 = S.Y1[j]; }
+            if (ix >= xa) {
+                const unsigned n = base + (unsigned)G.noff[k];
+                const bool bnd = !yzin || xbnd;
+                double y = bnd ? 0.0 : dadd(dadd(dadd(ac[k], y3.x), y2.x), y1.x);
+                if (fi_ap && (long long)n == fi_idx) y = flipbit(y, fi_bit);
+                const double pv = pc[k];
+                if (loop) part[0] = dfma(pv, y, part[0]);
+                if (d1) {
+                    part[1] = bnd ? dfma(0.0, y, part[1]) : dadd(part[1], y);
+                    part[2] = dfma(wv[k], pv, part[2]);
+                    part[3] = dfma(pv, pv, part[3]);
+                }
+                if (MODE == 0 && rhs) y = dfma(a.dtF, fv[k], y);
+                a.y[n] = y;
+                if (TWO || MODE == 1) pout[n] = pv;
+            }
+            an[k] = yzin ? dadd(dadd(dadd(an[k], y3.y), y2.y), y1.y) : 0.0;
+        }
+        ld_w(ix + 1);
+    };
+
+    // plane xa-1, then the inputs of plane xa and the coefficients of layer xa-1
+    ld_raw(xa - 1);
+    form(xa - 1, pA);
+#pragma unroll
+    for (int k = 0; k < SK; ++k) { S.P[0][tid + k * ST] = pA[k]; aA[k] = 0.0; aB[k] = 0.0; }
+    ld_raw(xa);
+    ld_coef(xa - 1);
+    for (int ix = xa - 1; ix <= xb; ++ix) {
+        layer(ix, (ix - xa + 1) & 1, pA, pB, aA, aB);
+#pragma unroll
+        for (int k = 0; k < SK; ++k) { pA[k] = pB[k]; aA[k] = aB[k]; }
+    }
+}
+
+// Colored operator: tile blockIdx.x of the slab partition (every node of the
+// grid belongs to exactly one tile; boundary nodes are projected to zero).
+// LOOP: the PCG-loop role (p formed in the kernel); otherwise the roles that
+// apply the operator to a given vector.
+template <int FORM, bool LOOP>
+__global__ void __launch_bounds__(ST, FORM == FORM_WHT ? 2 : 1) k_apply_slab(ApplyArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SlabSmem& S = *reinterpret_cast<SlabSmem*>(smem_raw);
+    DevState* st = a.st;
+    int fi_p = 0, fi_ap = 0, fi_r = 0, fi_bit = 0;
+    long long fi_idx = -1, fi_elem = -1;
+    const bool d1 = a.d1 != 0;
+    double part[MAXQ] = {0.0, 0.0, 0.0, 0.0};
+    const SlabTile T = slab_tile(a.part, blockIdx.x);
+    const SlabPos G = slab_pos(a.part, T, threadIdx.x);
+    if (LOOP) {
+        if (st->done) return;
+        const int iter = st->iter;
+        const double beta = st->beta;
+        const double* src_b = (iter > 0) ? ((iter & 1) ? a.pbuf0 : a.pbuf1) : nullptr;
+        double* pout = (iter & 1) ? a.pbuf1 : a.pbuf0;
+        if (st->fi_vec && st->fi_iter == iter) {
+            fi_idx = st->fi_idx; fi_bit = st->fi_bit;
+            fi_p = (st->fi_vec == FI_P); fi_ap = (st->fi_vec == FI_AP);
+        }
+        if (!src_b)
+            slab_march<FORM, 1>(a, S, T, G, a.z, src_b, beta, pout, true, d1, false, fi_p, fi_ap, 0, fi_bit, fi_idx,
+                                -1, part);
+        else if (fi_p || fi_ap)
+            slab_march<FORM, 2, true>(a, S, T, G, a.z, src_b, beta, pout, true, d1, false, fi_p, fi_ap, 0, fi_bit,
+                                      fi_idx, -1, part);
+        else
+            slab_march<FORM, 2, false>(a, S, T, G, a.z, src_b, beta, pout, true, d1, false, 0, 0, 0, 0, -1, -1, part);
+    } else {
+        if (a.role == ROLE_X0 && st->fi_armR) { fi_r = 1; fi_elem = st->fi_elem; fi_bit = st->fi_bit; }
+        const bool rhs = (a.role == ROLE_RHS) && a.F != nullptr;
+        slab_march<FORM, 0>(a, S, T, G, a.x, nullptr, 0.0, nullptr, false, d1, rhs, 0, 0, fi_r, fi_bit, -1, fi_elem,
+                            part);
+        if (!d1) return;
+    }
+    store_partials<MAXQ>(part, a.partials, a.part.nblk, S.sh);
+}
 
 // The D1 checksum (relative mismatch of 1_int.(Ax) and w.x) of an operator
 // application outside the PCG loop, once its partials are complete.  The loop
@@ -645,7 +853,7 @@ __global__ void k_absdiff_count(long long Nn, const double* a, const double* b, 
 
 // ---- node-parallel operator (every node, any projection) -------------------------
 // Recomputes the eight elements around each node; bit-identical node values to
-// k_apply_col (same element arithmetic, same summation order).  Used for
+// k_apply_slab (same element arithmetic, same summation order).  Used for
 // the unprojected set-up applies and the diagonal.
 enum GenKind { GEN_APPLY = 0, GEN_DIAG = 1 };
 struct GenArgs {
@@ -763,11 +971,9 @@ __global__ void __launch_bounds__(RT) k_apply_atomic(AtomArgs a) {
 }
 
 // After an atomic scatter: projection, p.Ap / D1 partials and role logic, on
-// the COL partition (p formed beforehand by k_form_p): thread l of tile
-// blockIdx.x visits the nodes its lane owns in the operator kernel, in the
-// same order, so the partials follow the same canonical order.
+// the canonical partition (p formed beforehand by k_form_p).
 struct FinishArgs {
-    ColLayout cp;
+    Part part;
     int N, role, d1, pad;
     const double* p;     // the vector the operator was applied to (roles other than LOOP)
     const double* pbuf0; // LOOP: p_k in pbuf[k & 1]
@@ -780,10 +986,11 @@ struct FinishArgs {
     unsigned* ticket;
     DevState* st;
 };
-__global__ void __launch_bounds__(RT) k_finish_atomic(FinishArgs a) {
+__global__ void __launch_bounds__(ST) k_finish_atomic(FinishArgs a) {
     __shared__ double sh[MAXQ][8];
     DevState* st = a.st;
-    const int N = a.N, NN = N + 1;
+    const int N = a.N;
+    const Part& P = a.part;
     int fi_ap = 0, fi_bit = 0;
     long long fi_idx = -1;
     int iter = 0;
@@ -795,21 +1002,16 @@ __global__ void __launch_bounds__(RT) k_finish_atomic(FinishArgs a) {
     const double* p = (a.role == ROLE_LOOP) ? ((iter & 1) ? a.pbuf1 : a.pbuf0) : a.p;
     const bool rhs = (a.role == ROLE_RHS) && a.F != nullptr;
     double part[MAXQ] = {0.0, 0.0, 0.0, 0.0};
-    const long long wt = (long long)blockIdx.x * CW + (threadIdx.x >> 5);
-    const ColLane C = col_lane(a.cp, wt, threadIdx.x & 31);
-    const bool own = (C.fl & 2u) && C.ec <= N;
-    const int c = C.ec;
-    for (int ix = C.xa; own && ix <= C.xb; ++ix) {
-        for (int j = 0; j <= CR; ++j) {
-            int r = C.r0 + j;
-            if (j == CR) {
-                if (!(C.fl & 4u)) continue;
-                r = N;
-            } else if (r > N) {
-                continue;
-            }
-            const long long n = ((long long)ix * NN + r) * NN + c;
-            const bool bnd = ix == 0 || ix == N || r == 0 || r == N || c == 0 || c == N;
+    const SlabTile T = slab_tile(P, blockIdx.x);
+    const SlabPos G = slab_pos(P, T, threadIdx.x);
+    const long long plane = (long long)P.NN * P.NN;
+    for (int ix = T.xa; ix <= T.xb; ++ix) {
+        const bool xbnd = ix == 0 || ix == N;
+#pragma unroll
+        for (int k = 0; k < SK; ++k) {
+            if (!sp_out(G.fl, k)) continue;
+            const long long n = (long long)ix * plane + G.noff[k];
+            const bool bnd = xbnd || sp_yzb(G.fl, k);
             double yv = bnd ? 0.0 : a.y[n];
             if (fi_ap && n == fi_idx) yv = flipbit(yv, fi_bit);
             const double pv = __ldg(p + n);
@@ -824,7 +1026,7 @@ __global__ void __launch_bounds__(RT) k_finish_atomic(FinishArgs a) {
         }
     }
     if (a.role != ROLE_LOOP && !a.d1) return;
-    store_partials<MAXQ>(part, a.partials, a.cp.ntiles, sh);
+    store_partials<MAXQ>(part, a.partials, P.nblk, sh);
 }
 
 // p_k = z (k = 0) or z + beta p_{k-1}, with the level-P fault (atomic path)

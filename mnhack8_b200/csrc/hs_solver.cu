@@ -74,8 +74,7 @@ struct hs_solver {
     hs_options opt{};
     int N = 0;
     long long Nn = 0, Ne = 0;
-    Part part{};                        // FLAT partition (vector update, reductions)
-    ColLayout cp{};                     // COL partition (operator kernel and its partials)
+    Part part{};
     RefMatrices mats{};
     ElemConsts ec{};
     double kmin = 0, kmax = 0, rhocmin = 0, rhocmax = 0;
@@ -136,36 +135,35 @@ hs_status sync_state_config(hs_solver* h, int max_iter, double tol) {
     return HS_OK;
 }
 
-int nblocks(const hs_solver* h) { return (int)h->cp.ntiles; }
+int nblocks(const hs_solver* h) { return (int)h->part.nblk; }
 
 // ---- operator launches -------------------------------------------------------------
 template <int FORM>
-bool set_col_smem() {
-    return cudaFuncSetAttribute(k_apply_col<FORM, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)kColSmem) == cudaSuccess &&
-           cudaFuncSetAttribute(k_apply_col<FORM, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)kColSmem) == cudaSuccess;
+bool set_smem_form() {
+    return cudaFuncSetAttribute(k_apply_slab<FORM, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kSlabSmem) == cudaSuccess &&
+           cudaFuncSetAttribute(k_apply_slab<FORM, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kSlabSmem) == cudaSuccess;
 }
-// the operator kernel's input ring exceeds the default 48 KB of dynamic shared memory
 bool set_smem_attributes() {
     static bool done = false, ok = true;
     if (done) return ok;
     done = true;
-    ok = set_col_smem<FORM_WHT>() && set_col_smem<FORM_FAST>() && set_col_smem<FORM_GAUSS>();
+    ok = set_smem_form<FORM_WHT>() && set_smem_form<FORM_FAST>() && set_smem_form<FORM_GAUSS>();
     return ok;
 }
 
 template <int FORM>
-void launch_col(hs_solver* h, const ApplyArgs& a) {
-    const int g = (int)h->cp.ntiles;
-    if (a.role == ROLE_LOOP) k_apply_col<FORM, true><<<g, RT, kColSmem, h->s>>>(a);
-    else k_apply_col<FORM, false><<<g, RT, kColSmem, h->s>>>(a);
+void launch_slab(hs_solver* h, const ApplyArgs& a) {
+    const int g = (int)h->part.ntiles;
+    if (a.role == ROLE_LOOP) k_apply_slab<FORM, true><<<g, ST, kSlabSmem, h->s>>>(a);
+    else k_apply_slab<FORM, false><<<g, ST, kSlabSmem, h->s>>>(a);
 }
 void launch_colored(hs_solver* h, const ApplyArgs& a) {
     switch (h->opt.kernel) {
-        case HS_KERNEL_WHT: launch_col<FORM_WHT>(h, a); break;
-        case HS_KERNEL_GAUSS: launch_col<FORM_GAUSS>(h, a); break;
-        default: launch_col<FORM_FAST>(h, a); break;
+        case HS_KERNEL_WHT: launch_slab<FORM_WHT>(h, a); break;
+        case HS_KERNEL_GAUSS: launch_slab<FORM_GAUSS>(h, a); break;
+        default: launch_slab<FORM_FAST>(h, a); break;
     }
 }
 void launch_nodes(hs_solver* h, const GenArgs& a) {
@@ -193,7 +191,7 @@ void apply_projected(hs_solver* h, int role, const double* x, double* y, double 
                      const double* w, const double* F, double dtF) {
     if (h->opt.scatter == HS_SCATTER_COLORED) {
         ApplyArgs a{};
-        a.cp = h->cp;
+        a.part = h->part;
         a.N = h->N; a.role = role; a.dt_eff = dt_eff;
         a.x = x; a.z = h->z.p; a.pbuf0 = h->p0.p; a.pbuf1 = h->p1.p;
         a.y = y; a.coef = h->coef.p; a.w = w; a.F = F; a.dtF = dtF;
@@ -202,7 +200,7 @@ void apply_projected(hs_solver* h, int role, const double* x, double* y, double 
         launch_colored(h, a);
         // the loop role's reductions are finished by the vector update (k_update)
         if (role != ROLE_LOOP && d1) {
-            FinalApplyArgs fa{h->partials.p, h->cp.ntiles, h->st.p, role, 1};
+            FinalApplyArgs fa{h->partials.p, h->part.nblk, h->st.p, role, 1};
             k_final_apply<<<1, RT, 0, h->s>>>(fa);
         }
         return;
@@ -217,13 +215,13 @@ void apply_projected(hs_solver* h, int role, const double* x, double* y, double 
     aa.y = y; aa.rhoc = h->rhoc.p; aa.kc = h->kc.p; aa.st = h->st.p; aa.ec = h->ec;
     launch_atomic(h, aa);
     FinishArgs f{};
-    f.cp = h->cp;
+    f.part = h->part;
     f.N = h->N; f.role = role; f.d1 = d1 ? 1 : 0; f.p = x; f.pbuf0 = h->p0.p; f.pbuf1 = h->p1.p;
     f.y = y; f.w = w; f.F = F; f.dtF = dtF;
     f.partials = h->partials.p; f.ticket = h->ticket.p; f.st = h->st.p;
     k_finish_atomic<<<nblocks(h), ST, 0, h->s>>>(f);
     if (role != ROLE_LOOP && d1) {
-        FinalApplyArgs fa{h->partials.p, h->cp.ntiles, h->st.p, role, 1};
+        FinalApplyArgs fa{h->partials.p, h->part.nblk, h->st.p, role, 1};
         k_final_apply<<<1, RT, 0, h->s>>>(fa);
     }
 }
@@ -233,7 +231,7 @@ void launch_update(hs_solver* h, int role, bool use_cond, cudaGraphConditionalHa
     u.Nn = h->Nn; u.nflat = h->part.nflat; u.role = role; u.x = h->T.p; u.b = h->b.p; u.r = h->r.p; u.z = h->z.p; u.Ap = h->Ap.p;
     u.d = h->diag.p; u.pbuf0 = h->p0.p; u.pbuf1 = h->p1.p; u.partials = h->upart.p; u.ticket = h->ticket.p;
     u.st = h->st.p; u.cond = cond; u.use_cond = 0;
-    u.d1 = h->opt.detect != 0; u.apart = h->partials.p; u.nblk = h->cp.ntiles;
+    u.d1 = h->opt.detect != 0; u.apart = h->partials.p; u.nblk = h->part.nblk;
     u.cond = cond; u.use_cond = use_cond ? 1 : 0;
     // one resident wave: the loop role sums the operator's partials once per CTA
     const long long wave = (long long)h->n_sm * kUpdateCtasPerSm;
@@ -352,8 +350,8 @@ const char* hs_last_error(void) { return hs::g_err.c_str(); }
 
 void hs_get_layout(int N, hs_layout_info* out) {
     if (!out) return;
-    const ColLayout L = col_layout(N);
-    out->cx = L.CX; out->ty = CR; out->tz = CSEG; out->rt = RT; out->bpt = CW; out->kf = KF;
+    const SlabLayout L = slab_layout(N);
+    out->cx = L.CX; out->ty = L.R; out->tz = L.C; out->rt = RT; out->bpt = SK; out->kf = KF;
 }
 
 hs_status hs_gaussian_ic(int N, double sigma, double* T_host) {
@@ -423,7 +421,6 @@ hs_status hs_create(const hs_options* opt, const double* k_host, const double* r
     h->Nn = (long long)(N + 1) * (N + 1) * (N + 1);
     h->Ne = (long long)N * N * N;
     h->part = make_part(N);
-    h->cp = col_layout(N);
     h->kmin = h->kmax = k_host[0];
     h->rhocmin = h->rhocmax = rhoc_host[0];
     for (long long e = 0; e < h->Ne; ++e) {
@@ -459,7 +456,7 @@ hs_status hs_create(const hs_options* opt, const double* k_host, const double* r
     HS_CUDA(h->diag.alloc(Nn)); HS_CUDA(h->F.alloc(Nn));
     HS_CUDA(h->T.alloc(Nn)); HS_CUDA(h->b.alloc(Nn)); HS_CUDA(h->r.alloc(Nn)); HS_CUDA(h->z.alloc(Nn));
     HS_CUDA(h->p0.alloc(Nn)); HS_CUDA(h->p1.alloc(Nn)); HS_CUDA(h->Ap.alloc(Nn));
-    HS_CUDA(h->partials.alloc((size_t)MAXQ * std::max(h->cp.ntiles, h->part.nflat) + 4096));
+    HS_CUDA(h->partials.alloc((size_t)MAXQ * std::max(h->part.nblk, h->part.nflat) + 4096));
     HS_CUDA(h->upart.alloc((size_t)3 * h->part.nflat + 256));
     HS_CUDA(h->ticket.alloc(1)); HS_CUDA(h->st.alloc(1)); HS_CUDA(h->red.alloc(8)); HS_CUDA(h->sp.alloc(2));
     HS_CUDA(cudaMemsetAsync(h->ticket.p, 0, sizeof(unsigned), h->s));

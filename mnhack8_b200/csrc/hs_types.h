@@ -77,66 +77,6 @@ inline SlabLayout slab_layout(int N) {
     return best;
 }
 
-// COL partition (the FP64 solver's operator kernel and its p.Ap / ABFT
-// partials, the APPLY order).  A warp is a unit of its own: its 32 lanes are
-// consecutive element columns ec = base-1+lane of one SEGMENT, each lane
-// marches CR node rows in y and the planes of one x-slab in x.  A lane owns
-// node column ec (the sum of its own element and, through a shuffle, its left
-// neighbour's) except the first lane of a segment, which only feeds its right
-// neighbour.  Full segments own 31 columns: segment s owns [31s, 31s+31); the
-// columns left over, [31S, N], form a partial segment of rem+1 lanes, and
-// floor(32/(rem+1)) partial segments (of consecutive row blocks) share a warp.
-// Row block rb owns node rows [rb*CR, rb*CR+CR) (those <= N); when (N+1) % CR
-// == 1 the last row block also owns row N ("extra" row) instead of a block of
-// one row.  Warp tasks of one x-slab: the full segments s-major (rb minor),
-// then the packed partial segments; task wt = xs*TPS + task.  A tile (CTA,
-// CW warps) takes tasks [CW*t, CW*t+CW).  Thread l = warp*32 + lane of tile t
-// accumulates its owned nodes plane by plane in increasing x, rows increasing
-// (the extra row last); the tile's RT values are combined by the block tree
-// below and the tile partials like every other partial.
-constexpr int CR = 4;                 // node rows per lane
-constexpr int CW = 8;                 // warps (tasks) per tile
-constexpr int CSEG = 31;              // columns owned by a full segment
-constexpr int COL_SLOTS = 148;        // co-resident tiles the layout assumes: one per SM (148 SMs)
-
-struct ColLayout {
-    int N, NN;
-    int S, rem, psize, P;   // full segments, columns of the partial one, its lanes, packed per warp
-    int NRB, extra;         // row blocks; the last also owns row N
-    int TPS;                // warp tasks per x-slab
-    int CX, NXB;            // planes per x-slab, x-slabs
-    long long ntasks, ntiles;
-};
-
-// The x-slab depth of an N-element grid: the CX minimising waves of
-// COL_SLOTS tiles x (4 (CR+1)(CX+1) + (CR+2)(CX+2)) (element rows and planes a
-// task computes, plus the rows it forms); ties keep the larger CX.
-inline ColLayout col_layout(int N) {
-    ColLayout L{};
-    L.N = N; L.NN = N + 1;
-    const int NN = N + 1;
-    L.S = NN / CSEG;
-    L.rem = NN - CSEG * L.S;
-    L.psize = L.rem > 0 ? L.rem + 1 : 0;
-    L.P = L.rem > 0 ? 32 / L.psize : 0;
-    if (NN % CR == 1 && NN > 1) { L.NRB = (NN - 1) / CR; L.extra = 1; }
-    else { L.NRB = (NN + CR - 1) / CR; L.extra = 0; }
-    L.TPS = L.S * L.NRB + (L.rem > 0 ? (L.NRB + L.P - 1) / L.P : 0);
-    long long best = -1;
-    for (int CX = NN; CX >= 1; --CX) {
-        const int NXB = (NN + CX - 1) / CX;
-        const long long ntasks = (long long)NXB * L.TPS;
-        const long long ntiles = (ntasks + CW - 1) / CW;
-        const long long waves = (ntiles + COL_SLOTS - 1) / COL_SLOTS;
-        const long long cost = waves * (4LL * (CR + 1) * (CX + 1) + (long long)(CR + 2) * (CX + 2));
-        if (best < 0 || cost < best) {
-            best = cost;
-            L.CX = CX; L.NXB = NXB; L.ntasks = ntasks; L.ntiles = ntiles;
-        }
-    }
-    return L;
-}
-
 constexpr int MAXQ = 4;               // reduced quantities per pass
 
 enum Form { FORM_FAST = 0, FORM_GAUSS = 1, FORM_WHT = 2 };

@@ -47,92 +47,67 @@ namespace {
 
 // ---- canonical reduction partitions (mirror the library's) --------------------
 // Two fixed orders.  The APPLY order (the operator kernel's p.Ap and ABFT
-// partials) follows the operator's column partition, described below.  The
-// FLAT order (every other reduction: the PCG vector dots, D2, E(t), plain
-// dots) cuts the node index range into blocks of RT*KF consecutive nodes,
-// thread t of block b accumulating the KF consecutive nodes b*RT*KF + t*KF + k,
+// partials) follows the operator's slab tiles, described below.  The FLAT
+// order (every other reduction: the PCG vector dots, D2, E(t), plain dots)
+// cuts the node index range into blocks of RT*KF consecutive nodes, thread t
+// of block b accumulating the KF consecutive nodes b*RT*KF + t*KF + k,
 // k = 0..KF-1, in order; blocks are combined like the apply order's partials.
 //
-// Column partition: work is cut into warp tasks of 32 lanes.  A lane holds an
-// element column ec of a SEGMENT of consecutive columns and owns node column
-// ec, except the first lane of a segment, which owns nothing.  Full segments
-// (S = (N+1)/31 of them) own 31 columns each, segment s starting at lane
-// column ec = 31s-1; the remaining rem = (N+1) - 31S columns form a partial
-// segment of rem+1 lanes starting at ec = 31S-1, and P = 32/(rem+1) partial
-// segments of consecutive row blocks are packed into one warp task (lanes
-// beyond P(rem+1) own nothing).  Row block rb owns node rows [CR*rb,
-// CR*rb+CR) that are <= N; when (N+1) % CR == 1 there are N/CR row blocks and
-// the last one also owns row N.  An x-slab xs owns planes [xs*CX, xs*CX+CX).
-// Tasks of one x-slab: the full segments s-major (row block minor), then the
-// packed partial segments; global task index xs*TPS + task.  Tile t takes
-// the tasks [CW*t, CW*t+CW); its thread l = w*32 + lane (w = task - CW*t)
-// accumulates its owned nodes plane by plane in increasing x, rows increasing
-// (the extra row N last).  A tile's RT values are combined by a 32-lane xor
+// Slab tiles: the node grid is cut into tiles of CX planes (x) x R rows (y) x
+// C columns (z), the last tile of each direction possibly short; tile
+// t = (tx*NRB + rb)*NCB + cb starts at plane tx*CX, row rb*R, column cb*C.  A
+// tile's RT threads own the positions j = l + k*RT (k = 0..SK-1) of a plane of
+// (R+2) x (C+2) positions (one halo row / column on each side), position j at
+// row rb*R - 1 + j/(C+2), column cb*C - 1 + j%(C+2); thread l accumulates the
+// tile's own nodes among its positions, plane by plane in increasing x and
+// positions in increasing k.  A block's RT values are combined by a 32-lane xor
 // butterfly per warp then an 8-way xor butterfly over warps; the tile
-// partials by RT strided sequential sums followed by the same block tree.
-// The x-slab depth CX is a fixed function of N, col_layout below.
+// partials are combined by RT strided sequential sums followed by the same
+// block tree.  (C, R, CX) is a fixed function of N, slab_layout below.
 const int RT = 256;
-const int CR = 4;                 // node rows per lane
-const int CW = 8;                 // warp tasks per tile
-const int CSEG = 31;              // columns owned by a full segment
-const int COL_SLOTS = 148;        // co-resident tiles the layout assumes
+const int SK = 4;                 // positions per thread
+const int SPOS = RT * SK;         // positions per tile plane, halo included
+const int SLAB_SLOTS = 296;       // co-resident tiles the layout assumes
 int g_KF = 2;                     // flat layout: consecutive nodes per thread
 
-struct ColLayout { int N, NN, S, rem, psize, P, NRB, extra, TPS, CX, NXB; long ntasks, ntiles; };
+struct SlabLayout { int C, R, CX, NCB, NRB, NXB; long ntiles; };
 
-// The library's x-slab depth: the CX minimising waves of COL_SLOTS tiles x
-// (4 (CR+1)(CX+1) + (CR+2)(CX+2)); ties keep the larger CX.
-ColLayout col_layout(int N) {
-    ColLayout L{};
-    L.N = N; L.NN = N + 1;
-    const int NN = N + 1;
-    L.S = NN / CSEG;
-    L.rem = NN - CSEG * L.S;
-    L.psize = L.rem > 0 ? L.rem + 1 : 0;
-    L.P = L.rem > 0 ? 32 / L.psize : 0;
-    if (NN % CR == 1 && NN > 1) { L.NRB = (NN - 1) / CR; L.extra = 1; }
-    else { L.NRB = (NN + CR - 1) / CR; L.extra = 0; }
-    L.TPS = L.S * L.NRB + (L.rem > 0 ? (L.NRB + L.P - 1) / L.P : 0);
-    long best = -1;
-    for (int CX = NN; CX >= 1; --CX) {
-        const int NXB = (NN + CX - 1) / CX;
-        const long ntasks = (long)NXB * L.TPS;
-        const long ntiles = (ntasks + CW - 1) / CW;
-        const long waves = (ntiles + COL_SLOTS - 1) / COL_SLOTS;
-        const long cost = waves * (4L * (CR + 1) * (CX + 1) + (long)(CR + 2) * (CX + 2));
-        if (best < 0 || cost < best) {
-            best = cost;
-            L.CX = CX; L.NXB = NXB; L.ntasks = ntasks; L.ntiles = ntiles;
+// The library's tile shape: among C >= min(N+1, 30) with (R+2)(C+2) <= SPOS
+// (R as large as that allows) and CX from the first waves of SLAB_SLOTS tiles,
+// the one minimising waves x (CX+2) x ((R+2)(C+2) + 2(R+1)(C+1)); ties keep the
+// smaller C, then fewer waves.
+SlabLayout slab_layout(int N) {
+    const long NN = N + 1;
+    SlabLayout best{};
+    long best_cost = -1;
+    const long cmin = NN < 30 ? NN : 30;
+    for (long C = cmin; C <= NN; ++C) {
+        const long Cw = C + 2;
+        const long Rmax = SPOS / Cw - 2;
+        if (Rmax < 1) break;
+        const long R = Rmax < NN ? Rmax : NN;
+        const long NCB = (NN + C - 1) / C, NRB = (NN + R - 1) / R, tyz = NCB * NRB;
+        const long work = Cw * (R + 2) + 2 * (C + 1) * (R + 1);
+        const long w0 = (tyz + SLAB_SLOTS - 1) / SLAB_SLOTS;
+        for (long w = w0; w < w0 + 4; ++w) {
+            long nx = w * SLAB_SLOTS / tyz;
+            if (nx < 1) continue;
+            if (nx > NN) nx = NN;
+            const long CX = (NN + nx - 1) / nx;
+            const long NXB = (NN + CX - 1) / CX;
+            const long waves = (tyz * NXB + SLAB_SLOTS - 1) / SLAB_SLOTS;
+            const long cost = waves * (CX + 2) * work;
+            if (best_cost < 0 || cost < best_cost) {
+                best_cost = cost;
+                best.C = (int)C; best.R = (int)R; best.CX = (int)CX;
+                best.NCB = (int)NCB; best.NRB = (int)NRB; best.NXB = (int)NXB;
+                best.ntiles = tyz * NXB;
+            }
         }
     }
-    return L;
+    return best;
 }
-
-// owned nodes of lane `lane` of warp task wt, in accumulation order
-template <class F>
-void col_owned(const ColLayout& L, long wt, int lane, F visit) {
-    if (wt >= L.ntasks) return;
-    const int xs = (int)(wt / L.TPS), task = (int)(wt % L.TPS);
-    int rb, sl, base;
-    if (task < L.S * L.NRB) {
-        rb = task % L.NRB; sl = lane; base = CSEG * (task / L.NRB) - 1;
-    } else {
-        const int k = task - L.S * L.NRB, slot = lane / L.psize;
-        sl = lane % L.psize; rb = k * L.P + slot; base = CSEG * L.S - 1;
-        if (slot >= L.P || rb >= L.NRB) return;
-    }
-    const int c = base + sl;
-    if (sl < 1 || c > L.N) return;
-    const int xa = xs * L.CX, xb = std::min(xa + L.CX, L.NN) - 1;
-    const bool extra = L.extra && rb == L.NRB - 1;
-    for (int x = xa; x <= xb; ++x) {
-        for (int j = 0; j < CR; ++j) {
-            const int r = rb * CR + j;
-            if (r <= L.N) visit(x, r, c);
-        }
-        if (extra) visit(x, L.N, c);
-    }
-}
+SlabLayout g_slab_override{};     // or_set_layout: a fixed tile shape (C > 0) instead of slab_layout(N)
 
 inline double tree256(const double* v) {
     double ws[8];
@@ -388,14 +363,30 @@ struct Oracle {
     // ---- canonical reduction ---------------------------------------------------
     template <class Term>
     double creduce(Term term) const {
-        const ColLayout L = col_layout(N);
+        SlabLayout L = slab_layout(N);
+        if (g_slab_override.C > 0) {
+            L = g_slab_override;
+            L.NCB = (NN + L.C - 1) / L.C; L.NRB = (NN + L.R - 1) / L.R; L.NXB = (NN + L.CX - 1) / L.CX;
+            L.ntiles = (long)L.NCB * L.NRB * L.NXB;
+        }
+        const int Cw = L.C + 2, Rw = L.R + 2;
         std::vector<double> P(L.ntiles);
         #pragma omp parallel for schedule(static)
         for (long t = 0; t < L.ntiles; ++t) {
+            const int cb = (int)(t % L.NCB), rb = (int)((t / L.NCB) % L.NRB), tx = (int)(t / ((long)L.NCB * L.NRB));
+            const int y0 = rb * L.R, z0 = cb * L.C, xa = tx * L.CX, xb = std::min(xa + L.CX, NN) - 1;
             double v[RT];
             for (int l = 0; l < RT; ++l) {
                 double acc = 0.0;
-                col_owned(L, t * CW + l / 32, l % 32, [&](int x, int r, int c) { acc = term(nid(x, r, c), acc); });
+                for (int ix = xa; ix <= xb; ++ix)
+                    for (int k = 0; k < SK; ++k) {
+                        const int j = l + k * RT;
+                        if (j >= Rw * Cw) continue;
+                        const int lr = j / Cw, lc = j % Cw;
+                        const int iy = y0 - 1 + lr, iz = z0 - 1 + lc;
+                        if (lr < 1 || lr > L.R || lc < 1 || lc > L.C || iy > N || iz > N) continue;
+                        acc = term(nid(ix, iy, iz), acc);
+                    }
                 v[l] = acc;
             }
             P[t] = tree256(v);
@@ -621,37 +612,18 @@ struct or_step_out {
     int snap;  // 1 if this step was a snapshot
 };
 
-// the flat order's nodes per thread kf (the apply order is the library's
-// per-N column partition; cx, ty and tz are accepted for the ABI and unused)
+// apply tile shape (cx planes, ty rows, tz columns; 0 = the per-N shape) and the
+// flat order's nodes per thread kf
 void or_set_layout(int cx, int ty, int tz, int kf) {
-    (void)cx; (void)ty; (void)tz;
+    g_slab_override = SlabLayout{};
+    if (cx > 0 && ty > 0 && tz > 0) { g_slab_override.C = tz; g_slab_override.R = ty; g_slab_override.CX = cx; }
     g_KF = kf;
 }
-// the per-N column partition: out[0..2] = cx (planes per x-slab), ty (node rows
-// per lane), tz (columns per full segment); returns the tile count
+// the per-N tile shape: out[0..2] = cx, ty (rows), tz (columns); returns the tile count
 long or_slab_layout(int N, int* out3) {
-    const ColLayout L = col_layout(N);
-    out3[0] = L.CX; out3[1] = CR; out3[2] = CSEG;
+    const SlabLayout L = slab_layout(N);
+    out3[0] = L.CX; out3[1] = L.R; out3[2] = L.C;
     return L.ntiles;
-}
-
-// 1 if every node of an N-element grid is owned by exactly one lane of the
-// column partition (and no lane owns a node outside the grid)
-int or_col_check(int N) {
-    const ColLayout L = col_layout(N);
-    const long NN = N + 1;
-    std::vector<unsigned char> cnt((size_t)(NN * NN * NN), 0);
-    bool ok = true;
-    for (long wt = 0; wt < L.ntiles * CW; ++wt)
-        for (int lane = 0; lane < 32; ++lane)
-            col_owned(L, wt, lane, [&](int x, int r, int c) {
-                if (x < 0 || x > N || r < 0 || r > N || c < 0 || c > N) { ok = false; return; }
-                unsigned char& k = cnt[(size_t)((x * NN + r) * NN + c)];
-                if (k) ok = false;
-                k = 1;
-            });
-    for (unsigned char k : cnt) ok = ok && k == 1;
-    return ok ? 1 : 0;
 }
 
 int or_set_threads(int n) {

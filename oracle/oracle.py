@@ -64,8 +64,6 @@ def lib():
         L.or_set_layout.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int]
         L.or_slab_layout.restype = C.c_long
         L.or_slab_layout.argtypes = [C.c_int, C.POINTER(C.c_int)]
-        L.or_col_check.restype = C.c_int
-        L.or_col_check.argtypes = [C.c_int]
         L.or_set_threads.restype = C.c_int
         L.or_set_threads.argtypes = [C.c_int]
         L.or_initial_condition.argtypes = [vp, dp]
@@ -78,23 +76,18 @@ def _ptr(a):
 
 
 def set_layout(cx: int = 0, ty: int = 0, tz: int = 0, kf: int = 2) -> None:
-    """Canonical reduction orders: the flat order's nodes per thread kf.  The
-    apply order is always the library's per-N column partition (cx, ty, tz are
-    kept for the call's signature and ignored)."""
+    """Canonical reduction orders: the apply order's slab tile (planes cx, rows
+    ty, columns tz; all 0 for the library's per-N shape slab_layout(N)) and
+    the flat order's nodes per thread kf.  The defaults are the library's; a
+    block has 256 threads of 4 positions each."""
     lib().or_set_layout(cx, ty, tz, kf)
 
 
 def slab_layout(N: int) -> dict:
-    """The per-N apply partition: planes per x-slab cx, node rows per lane ty,
-    columns per full warp segment tz, and the tile count."""
+    """The per-N apply tile shape: planes cx, rows ty, columns tz, and the tile count."""
     out = (C.c_int * 3)()
     nt = lib().or_slab_layout(int(N), out)
     return dict(cx=out[0], ty=out[1], tz=out[2], ntiles=int(nt))
-
-
-def col_coverage(N: int) -> int:
-    """1 if the apply partition of an N-element grid owns every node exactly once."""
-    return int(lib().or_col_check(int(N)))
 
 
 def set_threads(n: int) -> int:

@@ -2,10 +2,8 @@
 (ln32 field, seed 7; N=32, t 0.02, dt 5e-4, --kernel fast --scatter colored
 --detect --snap 1, fault at step 10 in element (16,16,16)) run through
 heat_solver_b200's entry point.  The files the reference's validation scripts
-parse carry the reference's recorded values to their printed digits (E(t)
-to its 11 digits within one unit of the last)."""
+parse carry the reference's recorded values to their printed digits."""
 import csv
-import math
 import os
 
 import numpy as np
@@ -33,13 +31,9 @@ def test_v6_level_R_case_through_the_cli(tmp_path, golden):
     assert len(trace) == len(g["trace"]) == 40
     assert set(g["trace"][0]) <= set(trace[0])           # every column the reference recorded
     for want, got in zip(g["trace"], trace):
-        for key in ("step", "spread_F", "cg_A", "cg_F", "d2_resid_A", "d2_resid_F", "d3_tmin_F", "d3_tmax_F"):
+        for key in ("step", "E_fault", "spread_F", "cg_A", "cg_F", "d2_resid_A", "d2_resid_F", "d3_tmin_F",
+                    "d3_tmax_F"):
             assert got[key] == want[key], (want["step"], key)
-        # E(t): 11 printed digits, the last within one unit (the recorded run
-        # summed its reductions in another order; E is a difference of two runs)
-        w = float(want["E_fault"])
-        unit = 10.0 ** (math.floor(math.log10(abs(w))) - 10) if w else 0.0
-        assert abs(float(got["E_fault"]) - w) <= 1.5 * unit, (want["step"], got["E_fault"], want["E_fault"])
         if want["step"] == sm["fi_step"]:
             assert got["d1_abft_F"] == want["d1_abft_F"]
     with open(out / "fi_summary_det.csv") as f:
