@@ -70,6 +70,9 @@ def parse():
                     help="instances of the supplementary batching measurement (0: skip)")
     ap.add_argument("--profile", action="store_true",
                     help="only the timed trajectories (no e2e, kernel timing or CPU baseline): for ncu captures")
+    ap.add_argument("--measure-traffic", action=argparse.BooleanOptionalAction, default=True,
+                    help="take roofline.traffic from a one-pass ncu capture of the operator kernel at --N "
+                         "(two DRAM counters, run after the same command exited 0 without ncu)")
     ap.add_argument("--profile-kernel", action="store_true",
                     help="only a few launches of the PCG operator kernel at --N (L2 scrubbed before each): "
                          "for one-launch ncu captures")
@@ -117,18 +120,54 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def profile_traffic(N):
-    """dram bytes per launch of the PCG operator kernel from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", f"k_apply_slab_loop_N{N}.md")
-    if not os.path.exists(p):
-        return None
-    for line in open(p):
-        if line.startswith("traffic_bytes_per_launch:"):
-            try:
-                return float(line.split(":", 1)[1].strip())
-            except ValueError:
-                return None
-    return None
+def measure_traffic(N, args):
+    """DRAM bytes (read + write) per launch of the PCG operator kernel, from one
+    ncu capture of `bench.py --profile-kernel` at this N taken by this run:
+    the command first runs without ncu and must exit 0, then ncu collects
+    only dram__bytes_read.sum and dram__bytes_write.sum (one pass, no memory
+    save/restore, clocks untouched) over the timed launches.  Returns (bytes
+    per launch or None, a note saying where the figure came from)."""
+    import csv
+    import io
+    import shutil
+    cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--N", str(N), "--profile-kernel",
+           "--kernel", args.kernel, "--scatter", args.scatter] + (["--no-detect"] if args.no_detect else [])
+    try:
+        plain = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+    except subprocess.TimeoutExpired:
+        return None, "not measured: the uncaptured kernel run did not finish"
+    if plain.returncode != 0:
+        return None, "not measured: the uncaptured kernel run failed"
+    ncu = shutil.which("ncu") or "/usr/local/cuda/bin/ncu"
+    if not os.path.exists(ncu):
+        return None, "not measured: ncu not found"
+    prof = [ncu, "--metrics", "dram__bytes_read.sum,dram__bytes_write.sum", "--clock-control", "none",
+            "-k", "regex:k_apply_slab", "--print-units", "base", "--csv"] + cmd
+    try:
+        out = subprocess.run(prof, capture_output=True, text=True, timeout=1800)
+    except subprocess.TimeoutExpired:
+        return None, "not measured: the ncu capture did not finish"
+    lines = out.stdout.splitlines()
+    head = next((i for i, l in enumerate(lines) if '"Metric Name"' in l), None)
+    if out.returncode != 0 or head is None:
+        return None, "not measured: " + ((out.stdout + out.stderr).strip().splitlines() or ["ncu failed"])[-1][:200]
+    per = {}
+    for row in csv.DictReader(io.StringIO("\n".join(lines[head:]))):
+        if "k_apply_slab" not in row.get("Kernel Name", ""):
+            continue
+        try:
+            v = float(row["Metric Value"].replace(",", ""))
+        except (KeyError, ValueError):
+            continue
+        per.setdefault(row["ID"], 0.0)
+        per[row["ID"]] += v
+    if not per:
+        return None, "not measured: no k_apply_slab launch in the capture"
+    ids = sorted(per, key=int)[-PROFILE_REPS:]          # the timed launches
+    vals = sorted(per[i] for i in ids)
+    return vals[len(vals) // 2], (f"ncu dram__bytes_read.sum + dram__bytes_write.sum, median of the last "
+                                  f"{len(ids)} k_apply_slab launches of `bench.py --N {N} --profile-kernel`, "
+                                  f"captured by this run")
 
 
 class ClockSampler:
@@ -357,7 +396,8 @@ def main():
     alg_k2 = 64 * nodes                                     # read x, p, Ap, r, d; write x, r, z
     peak, peak_kind = peaks()
     ach = alg_k1 / (ms_k1 * 1e-3) / 1e9
-    traffic = profile_traffic(N)
+    traffic, traffic_src = measure_traffic(N, args) if (world == 1 and args.measure_traffic) else \
+        (None, "not measured in this run (a 1-GPU bench.py --measure-traffic takes it)")
     iters_per_traj = it_all / max(1, world) / args.steps
     # per time step: step begin/end, RHS and x0 operator (+ final each with ABFT),
     # PCG prologue (update + final); per CG iteration: operator, update (which
@@ -374,7 +414,7 @@ def main():
         "config": workload_config(args, world),
         "cg_iters_per_trajectory": iters_per_traj,
         "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                     "traffic": traffic, "kernel": "k_apply_slab (PCG operator: p = z + beta p, Ap = A p, "
+                     "traffic": traffic, "traffic_source": traffic_src, "kernel": "k_apply_slab (PCG operator: p = z + beta p, Ap = A p, "
                      "p.Ap and ABFT partials)", "alg_bytes_per_launch": alg_k1, "ms_per_launch": ms_k1,
                      "peak_source": f"{peak_kind} hbm_gbs", "l2": "flushed before each timed launch",
                      "update_kernel": {"ms_per_launch": ms_k2, "alg_bytes_per_launch": alg_k2,
@@ -403,6 +443,7 @@ def main():
 
 
 GATE_N = 256
+PROFILE_REPS = 3
 
 
 def profile_kernel(args):
@@ -413,7 +454,7 @@ def profile_kernel(args):
     k, r = make_field(N, 1)
     g = _lib.Solver(N, DT, k, r, kernel=args.kernel, scatter=args.scatter, detect=not args.no_detect,
                     no_source=True, ic="gaussian", ic_sigma=IC_SIGMA, rtol=RTOL, max_iter=500, device=0)
-    ms = g.time_kernel(0, reps=3)
+    ms = g.time_kernel(0, reps=PROFILE_REPS)
     g.close()
     alg = (40 if not args.no_detect else 32) * (N + 1) ** 3 + 16 * N ** 3
     print(json.dumps({"N": N, "ms_per_launch": ms, "alg_bytes_per_launch": alg,
