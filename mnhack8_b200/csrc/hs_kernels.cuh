@@ -34,6 +34,16 @@ __device__ __forceinline__ double flipbit(double x, int bit) {
     return __longlong_as_double(__double_as_longlong(x) ^ (long long)(1ULL << bit));
 }
 
+// Programmatic dependent launch.  A kernel launched with programmatic stream
+// serialization may start while the kernel before it in the stream is still
+// running; pdl_wait() returns once that kernel has completed and its memory
+// operations are visible (a no-op for a kernel launched without the
+// attribute).  Everything a PCG-loop kernel reads that the loop writes comes
+// after it; before it a kernel only sets up geometry and reads loop-invariant
+// data.  pdl_release() lets the next kernel in the stream be scheduled early.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // ---- element operators; v[8] in q-order, in place --------------------------
 __device__ __forceinline__ void butterfly(double* v, int bit) {
 #pragma unroll
@@ -486,6 +496,8 @@ __global__ void __launch_bounds__(ST, FORM == FORM_WHT ? 2 : 1) k_apply_slab(App
     const SlabTile T = slab_tile(a.part, blockIdx.x);
     const SlabPos G = slab_pos(a.part, T, threadIdx.x);
     if (LOOP) {
+        pdl_wait();
+        pdl_release();
         if (st->done) return;
         const int iter = st->iter;
         const double beta = st->beta;
@@ -598,11 +610,15 @@ __device__ __forceinline__ void update_scalars(const UpdateArgs& a, const double
 // p.Ap is the same bits everywhere), and CTA 0 records p.Ap, alpha, the D1
 // checksum and a breakdown.
 //
-// It also finishes its own reductions: each flat block's partials are stored
-// at the block's index, and the last CTA to finish (an atomic ticket) combines
-// them in the FLAT order (final_sums) and runs the scalar logic, the work a
-// separate single-CTA kernel would do after it.
-constexpr int kUpdateCtasPerSm = 5;
+// It also finishes its own reductions, in the RUN order: CTA c of the
+// G = min(nflat, UPD_SLOTS) CTAs takes the consecutive flat blocks
+// [c nflat / G, (c+1) nflat / G) in order and sums their block partials, and
+// the last CTA to finish (an atomic ticket) combines the G run sums
+// (final_sums) and runs the scalar logic, the work a separate single-CTA
+// kernel would do after it.  G fits one resident wave (4 CTAs per SM), so the
+// last CTA's pass reads at most UPD_SLOTS partials per quantity.
+constexpr int kUpdateCtasPerSm = 4;
+static_assert(UPD_SLOTS == 148 * kUpdateCtasPerSm, "one resident wave of update CTAs on 148 SMs");
 __global__ void __launch_bounds__(RT, kUpdateCtasPerSm) k_update(UpdateArgs a) {
     static_assert(KF % 2 == 0, "pairs of nodes per thread");
     constexpr int NC = KF / 2;
@@ -612,6 +628,8 @@ __global__ void __launch_bounds__(RT, kUpdateCtasPerSm) k_update(UpdateArgs a) {
     DevState* st = a.st;
     const int tid = threadIdx.x;
     const bool pre = a.role == UPD_PRE;
+    pdl_wait();
+    pdl_release();
     if (!pre && st->done) {
         // the solve ended (converged, capped or broken down): end the graph's while loop
         if (a.use_cond && blockIdx.x == 0 && tid == 0) cudaGraphSetConditional(a.cond, 0u);
@@ -715,27 +733,30 @@ __global__ void __launch_bounds__(RT, kUpdateCtasPerSm) k_update(UpdateArgs a) {
             stv(a.x, xx); stv(a.r, rr); stv(a.z, dd);
         }
     };
-    // flat blocks blockIdx.x, + gridDim.x, ...; each block's partials at its own index
-    for (long long blk = blockIdx.x; blk < a.nflat; blk += gridDim.x) {
+    // run blockIdx.x of the RUN order: flat blocks [c nflat / G, (c+1) nflat / G),
+    // their partials summed in order from +0.0 (valid in thread 0)
+    const long long G = gridDim.x, c = blockIdx.x;
+    double run[3] = {0.0, 0.0, 0.0};
+    for (long long blk = c * a.nflat / G; blk < (c + 1) * a.nflat / G; ++blk) {
         double part[3] = {0.0, 0.0, 0.0};
         block(blk, part);
         cta_tree_sum<3>(part, sh);
-        if (tid == 0) {
 #pragma unroll
-            for (int q = 0; q < 3; ++q) a.partials[q * a.nflat + blk] = part[q];
-        }
+        for (int q = 0; q < 3; ++q) run[q] = dadd(run[q], part[q]);
     }
     if (tid == 0) {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) a.partials[q * G + c] = run[q];
         __threadfence();
         const unsigned t = atomicAdd(a.ticket, 1u);
         s_last = (t == gridDim.x - 1) ? 1u : 0u;
     }
     __syncthreads();
     if (!s_last) return;
-    // the last CTA: the FLAT order's final combination, then the scalar logic
+    // the last CTA: the run sums' final combination, then the scalar logic
     __threadfence();
     double v[3];
-    final_sums<3, 4>(v, a.partials, a.nflat, sh);     // short load batches keep the registers low
+    final_sums<3, 6>(v, a.partials, G, sh);            // load batches sized to the register budget
     if (tid == 0) {
         *a.ticket = 0u;
         update_scalars(a, v);

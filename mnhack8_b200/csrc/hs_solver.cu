@@ -153,17 +153,36 @@ bool set_smem_attributes() {
     return ok;
 }
 
+// Launch with programmatic stream serialization when pdl is set: the kernel's
+// CTAs may be scheduled while the previous kernel in the stream finishes, and
+// wait (pdl_wait) before reading what it wrote.  Used between the kernels of
+// the PCG loop, where it hides the launch gap.
+template <typename... KArgs, typename... Args>
+void launch_k(bool pdl, void (*k)(KArgs...), int grid, int block, size_t smem, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 template <int FORM>
-void launch_slab(hs_solver* h, const ApplyArgs& a) {
+void launch_slab(hs_solver* h, const ApplyArgs& a, bool pdl) {
     const int g = (int)h->part.ntiles;
-    if (a.role == ROLE_LOOP) k_apply_slab<FORM, true><<<g, ST, kSlabSmem, h->s>>>(a);
+    if (a.role == ROLE_LOOP) launch_k(pdl, k_apply_slab<FORM, true>, g, ST, kSlabSmem, h->s, a);
     else k_apply_slab<FORM, false><<<g, ST, kSlabSmem, h->s>>>(a);
 }
-void launch_colored(hs_solver* h, const ApplyArgs& a) {
+void launch_colored(hs_solver* h, const ApplyArgs& a, bool pdl) {
     switch (h->opt.kernel) {
-        case HS_KERNEL_WHT: launch_slab<FORM_WHT>(h, a); break;
-        case HS_KERNEL_GAUSS: launch_slab<FORM_GAUSS>(h, a); break;
-        default: launch_slab<FORM_FAST>(h, a); break;
+        case HS_KERNEL_WHT: launch_slab<FORM_WHT>(h, a, pdl); break;
+        case HS_KERNEL_GAUSS: launch_slab<FORM_GAUSS>(h, a, pdl); break;
+        default: launch_slab<FORM_FAST>(h, a, pdl); break;
     }
 }
 void launch_nodes(hs_solver* h, const GenArgs& a) {
@@ -188,7 +207,7 @@ void launch_atomic(hs_solver* h, const AtomArgs& a) {
 // Ap = A p).  Colored: one fused kernel.  Atomic: zero, element scatter with
 // atomics, then projection + partials on the canonical partition.
 void apply_projected(hs_solver* h, int role, const double* x, double* y, double dt_eff, bool d1,
-                     const double* w, const double* F, double dtF) {
+                     const double* w, const double* F, double dtF, bool pdl = false) {
     if (h->opt.scatter == HS_SCATTER_COLORED) {
         ApplyArgs a{};
         a.part = h->part;
@@ -197,7 +216,7 @@ void apply_projected(hs_solver* h, int role, const double* x, double* y, double 
         a.y = y; a.coef = h->coef.p; a.w = w; a.F = F; a.dtF = dtF;
         a.d1 = d1 ? 1 : 0;
         a.partials = h->partials.p; a.st = h->st.p; a.ec = h->ec;
-        launch_colored(h, a);
+        launch_colored(h, a, pdl);
         // the loop role's reductions are finished by the vector update (k_update)
         if (role != ROLE_LOOP && d1) {
             FinalApplyArgs fa{h->partials.p, h->part.nblk, h->st.p, role, 1};
@@ -226,16 +245,15 @@ void apply_projected(hs_solver* h, int role, const double* x, double* y, double 
     }
 }
 
-void launch_update(hs_solver* h, int role, bool use_cond, cudaGraphConditionalHandle cond = 0) {
+void launch_update(hs_solver* h, int role, bool use_cond, cudaGraphConditionalHandle cond = 0, bool pdl = false) {
     UpdateArgs u{};
     u.Nn = h->Nn; u.nflat = h->part.nflat; u.role = role; u.x = h->T.p; u.b = h->b.p; u.r = h->r.p; u.z = h->z.p; u.Ap = h->Ap.p;
     u.d = h->diag.p; u.pbuf0 = h->p0.p; u.pbuf1 = h->p1.p; u.partials = h->upart.p; u.ticket = h->ticket.p;
     u.st = h->st.p; u.cond = cond; u.use_cond = 0;
     u.d1 = h->opt.detect != 0; u.apart = h->partials.p; u.nblk = h->part.nblk;
     u.cond = cond; u.use_cond = use_cond ? 1 : 0;
-    // one resident wave: the loop role sums the operator's partials once per CTA
-    const long long wave = (long long)h->n_sm * kUpdateCtasPerSm;
-    k_update<<<(int)std::min<long long>(h->part.nflat, wave), RT, 0, h->s>>>(u);
+    // one CTA per run of the RUN order (one resident wave on B200)
+    launch_k(pdl, k_update, (int)std::min<long long>(h->part.nflat, UPD_SLOTS), RT, 0, h->s, u);
 }
 
 void launch_reduce(hs_solver* h, int kind, const double* a, const double* b, double* out) {
@@ -299,9 +317,11 @@ hs_status build_graph(hs_solver* h, int which) {
     const bool det = h->opt.detect != 0;
     // kLoopUnroll iterations per pass of the while body: every kernel returns at
     // once when the solve is done, and each final kernel sets the condition
+    // (programmatic launches between the body's kernels; the body's first kernel follows none)
+    const bool pdl = h->opt.scatter == HS_SCATTER_COLORED;
     for (int u = 0; u < kLoopUnroll; ++u) {
-        apply_projected(h, ROLE_LOOP, nullptr, h->Ap.p, h->opt.dt, det, h->wA.p, nullptr, 0.0);
-        launch_update(h, UPD_LOOP, true, cond);
+        apply_projected(h, ROLE_LOOP, nullptr, h->Ap.p, h->opt.dt, det, h->wA.p, nullptr, 0.0, pdl && u > 0);
+        launch_update(h, UPD_LOOP, true, cond, pdl);
     }
     HS_CUDA(cudaStreamEndCapture(h->s, &body));
     HS_CUDA(cudaGraphInstantiate(&h->gexec[which], g, 0));
@@ -625,9 +645,10 @@ hs_status pcg_direct(hs_solver* h, bool with_rhs) {
     const bool det = h->opt.detect != 0;
     DevState hsx{};
     for (int it = 0; it < (1 << 30); it += 16) {
+        const bool pdl = h->opt.scatter == HS_SCATTER_COLORED;
         for (int k = 0; k < 16; ++k) {
-            apply_projected(h, ROLE_LOOP, nullptr, h->Ap.p, h->opt.dt, det, h->wA.p, nullptr, 0.0);
-            launch_update(h, UPD_LOOP, false);
+            apply_projected(h, ROLE_LOOP, nullptr, h->Ap.p, h->opt.dt, det, h->wA.p, nullptr, 0.0, pdl && k > 0);
+            launch_update(h, UPD_LOOP, false, 0, pdl);
         }
         HS_CUDA(cudaMemcpyAsync(&hsx, h->st.p, sizeof(hsx), cudaMemcpyDeviceToHost, h->s));
         HS_CUDA(cudaStreamSynchronize(h->s));

@@ -14,10 +14,14 @@ namespace hs {
 // rb*R - 1 + lr, column cb*C - 1 + lc; thread t owns positions t + k*ST,
 // k = 0..SK-1.  A thread accumulates the tile nodes among its positions, plane
 // by plane in increasing x, positions in increasing k.
-// FLAT partition (every other reduction and the PCG vector update): blocks of
+// FLAT partition (the other reductions and the PCG vector update): blocks of
 // RT*KF consecutive nodes, thread t of block b taking the KF consecutive nodes
 // b*RT*KF + t*KF + k.
-// In both, a block combines its RT values by a 32-lane xor butterfly per warp
+// RUN order (the PCG vector update's b.b, r.z and r.r): the FLAT blocks'
+// partials summed sequentially from +0.0 in G = min(blocks, UPD_SLOTS) runs of
+// consecutive blocks, run c covering blocks [c*nb/G, (c+1)*nb/G); the run sums
+// are then combined like per-block partials.
+// In all, a block combines its RT values by a 32-lane xor butterfly per warp
 // and an 8-way xor butterfly over the warp sums, and a final pass combines the
 // per-block partials by RT strided sequential sums and the same block tree.
 // Every result is a fixed function of the inputs, independent of scheduling.
@@ -33,6 +37,7 @@ constexpr int ST = RT;                // threads per slab CTA
 constexpr int SK = 4;                 // positions per thread
 constexpr int SPOS = ST * SK;         // positions per plane of a slab CTA (halo included)
 constexpr int SLAB_SLOTS = 296;       // co-resident slab CTAs assumed by the layout: 148 SMs x 2
+constexpr int UPD_SLOTS = 592;        // runs of the RUN order: co-resident update CTAs, 148 SMs x 4
 
 struct SlabLayout {
     int C, R, CX;          // tile columns, rows, planes

@@ -48,7 +48,7 @@ namespace {
 // ---- canonical reduction partitions (mirror the library's) --------------------
 // Two fixed orders.  The APPLY order (the operator kernel's p.Ap and ABFT
 // partials) follows the operator's slab tiles, described below.  The FLAT
-// order (every other reduction: the PCG vector dots, D2, E(t), plain dots)
+// order (every other reduction: D2, E(t), plain dots)
 // cuts the node index range into blocks of RT*KF consecutive nodes, thread t
 // of block b accumulating the KF consecutive nodes b*RT*KF + t*KF + k,
 // k = 0..KF-1, in order; blocks are combined like the apply order's partials.
@@ -64,11 +64,14 @@ namespace {
 // butterfly per warp then an 8-way xor butterfly over warps; the tile
 // partials are combined by RT strided sequential sums followed by the same
 // block tree.  (C, R, CX) is a fixed function of N, slab_layout below.
+// The PCG vector update's dots (b.b, r.z, r.r) take the RUN order: the flat
+// blocks' partials first summed in runs of consecutive blocks (ureduce).
 const int RT = 256;
 const int SK = 4;                 // positions per thread
 const int SPOS = RT * SK;         // positions per tile plane, halo included
 const int SLAB_SLOTS = 296;       // co-resident tiles the layout assumes
 int g_KF = 2;                     // flat layout: consecutive nodes per thread
+const long UPD_SLOTS = 592;       // runs of the update order: co-resident update CTAs (148 SMs x 4)
 
 struct SlabLayout { int C, R, CX, NCB, NRB, NXB; long ntiles; };
 
@@ -399,8 +402,9 @@ struct Oracle {
         }
         return tree256(v);
     }
+    // flat blocks' partials (one per block of RT*KF consecutive nodes)
     template <class Term>
-    double freduce(Term term) const {
+    std::vector<double> fblocks(Term term) const {
         const long RB = (long)RT * g_KF;
         const long nb = (Nn + RB - 1) / RB;
         std::vector<double> P(nb);
@@ -418,6 +422,10 @@ struct Oracle {
             }
             P[b] = tree256(v);
         }
+        return P;
+    }
+    // partials combined: RT strided sequential sums, then the block tree
+    static double combine(const std::vector<double>& P) {
         double v[RT];
         for (int l = 0; l < RT; ++l) {
             double acc = 0.0;
@@ -426,8 +434,30 @@ struct Oracle {
         }
         return tree256(v);
     }
+    template <class Term>
+    double freduce(Term term) const { return combine(fblocks(term)); }
+    // RUN order (the PCG vector update's r.r, r.z and b.b): the flat blocks'
+    // partials summed sequentially from +0.0 in G = min(blocks, UPD_SLOTS) runs
+    // of consecutive blocks, run c covering blocks [c*nb/G, (c+1)*nb/G); the
+    // run sums combined like partials.
+    template <class Term>
+    double ureduce(Term term) const {
+        const std::vector<double> P = fblocks(term);
+        const long nb = (long)P.size();
+        const long G = nb < UPD_SLOTS ? nb : UPD_SLOTS;
+        std::vector<double> U(G);
+        for (long c = 0; c < G; ++c) {
+            double acc = 0.0;
+            for (long b = c * nb / G; b < (c + 1) * nb / G; ++b) acc = acc + P[b];
+            U[c] = acc;
+        }
+        return combine(U);
+    }
     double dot(const double* a, const double* b) const {
         return freduce([&](long n, double acc) { return std::fma(a[n], b[n], acc); });
+    }
+    double udot(const double* a, const double* b) const {   // update order
+        return ureduce([&](long n, double acc) { return std::fma(a[n], b[n], acc); });
     }
     double adot(const double* a, const double* b) const {   // apply order
         return creduce([&](long n, double acc) { return std::fma(a[n], b[n], acc); });
@@ -533,7 +563,7 @@ struct Oracle {
         armed_R = 0;
         double bb = 0, rz = 0, rr = 0;
         for (long n = 0; n < Nn; ++n) { r[n] = std::fma(-1.0, Ap[n], b[n]); z[n] = r[n] / diag[n]; }
-        bb = dot(b, b); rz = dot(r, z); rr = dot(r, r);
+        bb = udot(b, b); rz = udot(r, z); rr = udot(r, r);
         double bnorm = std::sqrt(bb);
         if (bnorm < 1e-30) bnorm = 1.0;
         if (log) log->rel0 = std::sqrt(rr) / bnorm;
@@ -565,7 +595,7 @@ struct Oracle {
             }
             if (vec_level == LV_RV && it == vec_iter) r[vec_idx] = flip(r[vec_idx], fi_bit);
             for (long n = 0; n < Nn; ++n) z[n] = r[n] / diag[n];
-            rr = dot(r, r); rz = dot(r, z);
+            rr = udot(r, r); rz = udot(r, z);
             double rnorm = std::sqrt(rr);
             bool conv = (rnorm / bnorm < tol);
             beta = 0.0;
