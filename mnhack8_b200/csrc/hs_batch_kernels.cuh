@@ -7,9 +7,11 @@
 // an FP32 Jacobi-PCG solve of A d = r to a loose relative tolerance (FP32
 // operator and preconditioner, FP64 dot products of the FP32 values), and
 // T += d in FP64, until ||b - A T|| / ||b|| < rtol.
-// The CG dot products, the outer residual and the ABFT checksum sums are
-// accumulated in FP64 with compensation (hs_csum.h): every partial is a pair
-// (hi, lo), stored as quantity q and q + NQ, and merged pair-wise.
+// The sums of the FP64 applies (the outer residual ||b - A T||, ||b||, the
+// ABFT checksum sums of the FP64 applies) and the inner solve's starting r.z
+// and r.r are accumulated in FP64 with compensation (hs_csum.h); the inner
+// FP32 iterations' sums are plain FP64 sums of FP32 values.  Every partial is
+// a pair (hi, lo), stored as quantity q and q + NQ, and merged pair-wise.
 #pragma once
 #include "hs_kernels.cuh"
 #include "hs_csum.h"
@@ -335,11 +337,23 @@ __device__ __forceinline__ void kb_tile(const BatchArgs& B, BSlabSmem<V>& S, lon
                     if (fi_ap && (long long)n == fi_idx) { y = flipf(y, fi_bit); st->fi_fired = 1; }
                 }
                 const double pv = (double)pc[k], yd = (double)y;
-                if (loop) csum_fma(part[0], pv, yd);
-                if (d1) {
-                    if (!bnd) csum_add(part[1], yd);
-                    csum_fma(part[2], wv[k], pv);
-                    part[3].hi = dfma(pv, pv, part[3].hi);      // the norm only scales the threshold
+                if constexpr (sizeof(V) == 8) {
+                    // FP64 applies (right-hand side, outer residual): compensated sums
+                    if (loop) csum_fma(part[0], pv, yd);
+                    if (d1) {
+                        if (!bnd) csum_add(part[1], yd);
+                        csum_fma(part[2], wv[k], pv);
+                        part[3].hi = dfma(pv, pv, part[3].hi);  // the norm only scales the threshold
+                    }
+                } else {
+                    // FP32 inner applies: FP64 sums of FP32 values; their rounding (~1e-16 n)
+                    // is far below the FP32 operator's own (~1e-9), so no compensation
+                    if (loop) part[0].hi = dfma(pv, yd, part[0].hi);
+                    if (d1) {
+                        if (!bnd) part[1].hi = dadd(part[1].hi, yd);
+                        part[2].hi = dfma(wv[k], pv, part[2].hi);
+                        part[3].hi = dfma(pv, pv, part[3].hi);
+                    }
                 }
                 __stwb(yout + n, y);                      // global stores (the pointers come from global memory)
                 if (loop) __stwb(pout + n, pc[k]);
@@ -570,8 +584,10 @@ __global__ void __launch_bounds__(RT) kb_update32(BatchArgs B) {
                 rv[k] = r;
                 zv[k] = __fmul_rn(r, iv[k]);
                 if (k < f.cnt) {
-                    csum_add(part[0], dmul((double)r, (double)r));         // exact products
-                    csum_add(part[1], dmul((double)r, (double)zv[k]));
+                    // products of FP32 values are exact in FP64; plain FP64 sums suffice
+                    // for the inner solve's 1e-4 relative tolerance
+                    part[0].hi = dfma((double)r, (double)r, part[0].hi);
+                    part[1].hi = dfma((double)r, (double)zv[k], part[1].hi);
                 }
             }
             if (f.cnt == 2) {

@@ -615,15 +615,16 @@ __device__ __forceinline__ void update_scalars(const UpdateArgs& a, const double
 // [c nflat / G, (c+1) nflat / G) in order and sums their block partials, and
 // the last CTA to finish (an atomic ticket) combines the G run sums
 // (final_sums) and runs the scalar logic, the work a separate single-CTA
-// kernel would do after it.  G fits one resident wave (4 CTAs per SM), so the
+// kernel would do after it.  G fits one resident wave (5 CTAs per SM), so the
 // last CTA's pass reads at most UPD_SLOTS partials per quantity.
-constexpr int kUpdateCtasPerSm = 4;
+constexpr int kUpdateCtasPerSm = 5;
 static_assert(UPD_SLOTS == 148 * kUpdateCtasPerSm, "one resident wave of update CTAs on 148 SMs");
 __global__ void __launch_bounds__(RT, kUpdateCtasPerSm) k_update(UpdateArgs a) {
     static_assert(KF % 2 == 0, "pairs of nodes per thread");
     constexpr int NC = KF / 2;
     __shared__ double sh[MAXQ][8];
     __shared__ double s_pAp;
+    __shared__ double s_run[3];
     __shared__ unsigned s_last;
     DevState* st = a.st;
     const int tid = threadIdx.x;
@@ -735,18 +736,22 @@ __global__ void __launch_bounds__(RT, kUpdateCtasPerSm) k_update(UpdateArgs a) {
     };
     // run blockIdx.x of the RUN order: flat blocks [c nflat / G, (c+1) nflat / G),
     // their partials summed in order from +0.0 (valid in thread 0)
-    const long long G = gridDim.x, c = blockIdx.x;
-    double run[3] = {0.0, 0.0, 0.0};
-    for (long long blk = c * a.nflat / G; blk < (c + 1) * a.nflat / G; ++blk) {
+    // (the running sums live in shared memory, written by thread 0 only)
+    const int G = gridDim.x, c = blockIdx.x;
+    if (tid == 0) { s_run[0] = 0.0; s_run[1] = 0.0; s_run[2] = 0.0; }
+    const int b1 = (int)((long long)(c + 1) * a.nflat / G);
+    for (int blk = (int)((long long)c * a.nflat / G); blk < b1; ++blk) {
         double part[3] = {0.0, 0.0, 0.0};
         block(blk, part);
         cta_tree_sum<3>(part, sh);
+        if (tid == 0) {
 #pragma unroll
-        for (int q = 0; q < 3; ++q) run[q] = dadd(run[q], part[q]);
+            for (int q = 0; q < 3; ++q) s_run[q] = dadd(s_run[q], part[q]);
+        }
     }
     if (tid == 0) {
 #pragma unroll
-        for (int q = 0; q < 3; ++q) a.partials[q * G + c] = run[q];
+        for (int q = 0; q < 3; ++q) a.partials[(long long)q * G + c] = s_run[q];
         __threadfence();
         const unsigned t = atomicAdd(a.ticket, 1u);
         s_last = (t == gridDim.x - 1) ? 1u : 0u;
@@ -756,7 +761,7 @@ __global__ void __launch_bounds__(RT, kUpdateCtasPerSm) k_update(UpdateArgs a) {
     // the last CTA: the run sums' final combination, then the scalar logic
     __threadfence();
     double v[3];
-    final_sums<3, 6>(v, a.partials, G, sh);            // load batches sized to the register budget
+    final_sums<3, 4>(v, a.partials, G, sh);            // one batch of loads per thread (G <= 740)
     if (tid == 0) {
         *a.ticket = 0u;
         update_scalars(a, v);

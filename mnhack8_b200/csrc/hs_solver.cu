@@ -277,6 +277,17 @@ void enqueue_pcg_prologue(hs_solver* h, bool with_rhs) {
 // (chunks of iterations, the device "done" flag read back between chunks)
 // instead of through the graph's while node: profilers cannot attribute
 // kernels that run inside a conditional graph node.
+// HS_PDL=0 launches the PCG loop's kernels without programmatic dependent
+// launch (each kernel starts after the previous one has finished).
+bool pdl_enabled() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("HS_PDL");
+        v = (e && e[0] == '0') ? 0 : 1;
+    }
+    return v == 1;
+}
+
 bool graphs_enabled() {
     static int v = -1;
     if (v < 0) {
@@ -318,7 +329,7 @@ hs_status build_graph(hs_solver* h, int which) {
     // kLoopUnroll iterations per pass of the while body: every kernel returns at
     // once when the solve is done, and each final kernel sets the condition
     // (programmatic launches between the body's kernels; the body's first kernel follows none)
-    const bool pdl = h->opt.scatter == HS_SCATTER_COLORED;
+    const bool pdl = h->opt.scatter == HS_SCATTER_COLORED && pdl_enabled();
     for (int u = 0; u < kLoopUnroll; ++u) {
         apply_projected(h, ROLE_LOOP, nullptr, h->Ap.p, h->opt.dt, det, h->wA.p, nullptr, 0.0, pdl && u > 0);
         launch_update(h, UPD_LOOP, true, cond, pdl);
@@ -645,7 +656,7 @@ hs_status pcg_direct(hs_solver* h, bool with_rhs) {
     const bool det = h->opt.detect != 0;
     DevState hsx{};
     for (int it = 0; it < (1 << 30); it += 16) {
-        const bool pdl = h->opt.scatter == HS_SCATTER_COLORED;
+        const bool pdl = h->opt.scatter == HS_SCATTER_COLORED && pdl_enabled();
         for (int k = 0; k < 16; ++k) {
             apply_projected(h, ROLE_LOOP, nullptr, h->Ap.p, h->opt.dt, det, h->wA.p, nullptr, 0.0, pdl && k > 0);
             launch_update(h, UPD_LOOP, false, 0, pdl);

@@ -37,7 +37,7 @@ constexpr int ST = RT;                // threads per slab CTA
 constexpr int SK = 4;                 // positions per thread
 constexpr int SPOS = ST * SK;         // positions per plane of a slab CTA (halo included)
 constexpr int SLAB_SLOTS = 296;       // co-resident slab CTAs assumed by the layout: 148 SMs x 2
-constexpr int UPD_SLOTS = 592;        // runs of the RUN order: co-resident update CTAs, 148 SMs x 4
+constexpr int UPD_SLOTS = 740;        // runs of the RUN order: co-resident update CTAs, 148 SMs x 5
 
 struct SlabLayout {
     int C, R, CX;          // tile columns, rows, planes

@@ -71,7 +71,7 @@ const int SK = 4;                 // positions per thread
 const int SPOS = RT * SK;         // positions per tile plane, halo included
 const int SLAB_SLOTS = 296;       // co-resident tiles the layout assumes
 int g_KF = 2;                     // flat layout: consecutive nodes per thread
-const long UPD_SLOTS = 592;       // runs of the update order: co-resident update CTAs (148 SMs x 4)
+const long UPD_SLOTS = 740;       // runs of the update order: co-resident update CTAs (148 SMs x 5)
 
 struct SlabLayout { int C, R, CX, NCB, NRB, NXB; long ntiles; };
 
