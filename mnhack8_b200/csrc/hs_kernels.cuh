@@ -611,8 +611,8 @@ __device__ __forceinline__ void update_scalars(const UpdateArgs& a, const double
 // checksum and a breakdown.
 //
 // It also finishes its own reductions, in the RUN order: CTA c of the
-// G = min(nflat, UPD_SLOTS) CTAs takes the consecutive flat blocks
-// [c nflat / G, (c+1) nflat / G) in order and sums their block partials, and
+// G = min(nflat, UPD_SLOTS) CTAs takes the flat blocks c, c+G, c+2G, ... in
+// order and sums their block partials, and
 // the last CTA to finish (an atomic ticket) combines the G run sums
 // (final_sums) and runs the scalar logic, the work a separate single-CTA
 // kernel would do after it.  G fits one resident wave (5 CTAs per SM), so the
@@ -734,13 +734,12 @@ __global__ void __launch_bounds__(RT, kUpdateCtasPerSm) k_update(UpdateArgs a) {
             stv(a.x, xx); stv(a.r, rr); stv(a.z, dd);
         }
     };
-    // run blockIdx.x of the RUN order: flat blocks [c nflat / G, (c+1) nflat / G),
-    // their partials summed in order from +0.0 (valid in thread 0)
-    // (the running sums live in shared memory, written by thread 0 only)
+    // run blockIdx.x of the RUN order: flat blocks c, c+G, ..., their partials
+    // summed in order from +0.0 (the running sums live in shared memory,
+    // written by thread 0 only)
     const int G = gridDim.x, c = blockIdx.x;
     if (tid == 0) { s_run[0] = 0.0; s_run[1] = 0.0; s_run[2] = 0.0; }
-    const int b1 = (int)((long long)(c + 1) * a.nflat / G);
-    for (int blk = (int)((long long)c * a.nflat / G); blk < b1; ++blk) {
+    for (int blk = c; blk < a.nflat; blk += G) {
         double part[3] = {0.0, 0.0, 0.0};
         block(blk, part);
         cta_tree_sum<3>(part, sh);

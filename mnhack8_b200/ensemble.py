@@ -325,6 +325,62 @@ def serving(n=400, rate=200.0, seed=11, rtol=1e-8, inner_tol=1e-4, max_live=64, 
 
 
 # ---- config 3: detection coverage of the mixed form, beside FP64 ------------------------
+FP32_D1_LAMBDA = 6.0        # tail factor of the probabilistic bound (false-alarm odds ~2 exp(-18) per check)
+FP32_D1_DEPTH = 16          # roundings on the path of one node output of the FP32 apply
+
+
+def checksum_weights(N, k, rhoc, dt):
+    """w = A 1_int and w_abs = |A| 1_int on the interior rows (the rows the
+    checksum 1_int . y sums), from the Q1 cube element matrices
+    M^ = m(x)m(x)m and K^ = k(x)m(x)m + m(x)k(x)m + m(x)m(x)k (m = h/6 [2 1; 1 2],
+    k = 1/h [1 -1; -1 1]); |A| takes the absolute value of every element
+    matrix entry.  Host NumPy, for the threshold below."""
+    h = 1.0 / N
+    m = h / 6.0 * np.array([[2.0, 1.0], [1.0, 2.0]])
+    kk = 1.0 / h * np.array([[1.0, -1.0], [-1.0, 1.0]])
+    M = np.kron(m, np.kron(m, m))
+    K = np.kron(kk, np.kron(m, m)) + np.kron(m, np.kron(kk, m)) + np.kron(m, np.kron(m, kk))
+    k3, r3 = np.asarray(k).reshape(N, N, N), np.asarray(rhoc).reshape(N, N, N)
+    inner = np.zeros((N + 1,) * 3)
+    inner[1:-1, 1:-1, 1:-1] = 1.0
+    corner = [((q >> 2) & 1, (q >> 1) & 1, q & 1) for q in range(8)]
+    mask = [inner[ox:ox + N, oy:oy + N, oz:oz + N] for ox, oy, oz in corner]
+    w, wabs = np.zeros((N + 1,) * 3), np.zeros((N + 1,) * 3)
+    for i, (ox, oy, oz) in enumerate(corner):
+        mr = sum(M[i, j] * mask[j] for j in range(8))
+        kr = sum(K[i, j] * mask[j] for j in range(8))
+        ma = sum(abs(M[i, j]) * mask[j] for j in range(8))
+        ka = sum(abs(K[i, j]) * mask[j] for j in range(8))
+        w[ox:ox + N, oy:oy + N, oz:oz + N] += r3 * mr + dt * k3 * kr
+        wabs[ox:ox + N, oy:oy + N, oz:oz + N] += r3 * ma + dt * k3 * ka
+    return w * inner, wabs * inner
+
+
+def fp32_d1_threshold(N, k, rhoc, dt, lam=FP32_D1_LAMBDA, depth=FP32_D1_DEPTH):
+    """D1 threshold of an FP32 apply from a probabilistic rounding-error bound.
+
+    D1 = |1_int . y^ - w . p| / (||w|| ||p||), y^ the FP32 apply of the FP32
+    vector p (the checksum sums themselves are FP64).  Each node output
+    carries `depth` roundings of unit u = 2^-24 (the WHT butterflies, the
+    eigenvalue scaling, the node sum, the coefficients rounded to FP32), each
+    at most u times a value bounded by (|A| |p|)_i.  Modelling them as
+    independent, mean-zero (Higham and Mary, SIAM J. Sci. Comput. 41 (2019)
+    A2815), their sum over the interior nodes stays below
+    lam sqrt(depth) u || |A| |p| ||_2 except with probability 2 exp(-lam^2/2).
+    For a field p that is smooth on the element scale, (|A| |p|)_i ~
+    w_abs,i |p_i|, and with |p| spread over the domain
+    || w_abs o p || ~ ||w_abs|| ||p|| / sqrt(n_int), so
+
+        D1 < lam sqrt(depth) u ||w_abs|| / (sqrt(n_int) ||w||).
+
+    The threshold is this bound: a fixed function of the problem (grid,
+    field, dt), with no input from a clean run."""
+    w, wabs = checksum_weights(N, k, rhoc, dt)
+    n_int = (N - 1) ** 3
+    return lam * np.sqrt(depth) * 2.0 ** -24 * float(np.linalg.norm(wabs)) / (
+        np.sqrt(n_int) * float(np.linalg.norm(w)))
+
+
 def coverage(N=64, steps=20, flips=1000, seed=21, per_batch=None, rtol=1e-8, inner_tol=1e-4, sigma=1.5,
              corr_frac=1.0 / 16.0, sig_err=1e-6, device=0, rows_out=None, fp64=True):
     """Seeded single-bit flips into the FP32 inner vectors of the mixed form
@@ -332,8 +388,10 @@ def coverage(N=64, steps=20, flips=1000, seed=21, per_batch=None, rtol=1e-8, inn
     step and inner iteration of the first correction uniform), run as batches
     of faulted copies of one problem, beside the FP64 drop-in's campaign
     (p, r, Ap, bits 0..63) on the same problem.  A mixed-form flip counts as
-    detected when an FP32 apply's D1 exceeds 100x the clean run's FP32 noise
-    floor, an FP64 apply's D1 exceeds 1e-10, or a step ends at the correction
+    detected when an FP32 apply's D1 exceeds the threshold of the
+    probabilistic rounding bound (fp32_d1_threshold; the clean run's FP32
+    noise floor is reported beside it), an FP64 apply's D1 exceeds 1e-10 (the
+    reference's rule), or a step ends at the correction
     cap or an inner solve goes non-finite (its correction is then discarded);
     it is significant when its final field error exceeds sig_err (or is not
     finite)."""
@@ -347,7 +405,7 @@ def coverage(N=64, steps=20, flips=1000, seed=21, per_batch=None, rtol=1e-8, inn
         pass
     T_clean, clean = b.field(s), b.info(s)
     b.close()
-    thr32 = max(100.0 * clean["d1_max32"], 1e-12)
+    thr32 = fp32_d1_threshold(N, k, r, DT)
     if per_batch is None:
         # faulted copies per batch: at most 125, within 60 % of the free HBM
         import torch
@@ -397,7 +455,9 @@ def coverage(N=64, steps=20, flips=1000, seed=21, per_batch=None, rtol=1e-8, inn
         "abft_d1_rate_of_fired": share(lambda x: x["d1_max32"] > thr32, fired),
         "max_err_of_undetected": max([x["err"] for x in fired if not x["detected"]] or [0.0]),
         "median_extra_inner_iters": float(np.median([x["extra_inner"] for x in fired])) if fired else None,
-        "fp32_noise_floor_max_d1": clean["d1_max32"], "fp32_threshold": thr32, "wall_s": wall,
+        "fp32_noise_floor_max_d1": clean["d1_max32"], "fp32_threshold": thr32,
+        "fp32_threshold_rule": f"probabilistic rounding bound, lambda {FP32_D1_LAMBDA:g}, depth {FP32_D1_DEPTH}",
+        "clean_run_false_alarm": bool(clean["d1_max32"] > thr32), "wall_s": wall,
         "by_vector": {v: {"fired": sum(1 for x in fired if x["level"] == lv),
                           "detected_rate": share(lambda x: x["detected"], [x for x in fired if x["level"] == lv])}
                       for v, lv in (("p", 5), ("r", 6), ("Ap", 7))},

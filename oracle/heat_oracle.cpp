@@ -437,9 +437,9 @@ struct Oracle {
     template <class Term>
     double freduce(Term term) const { return combine(fblocks(term)); }
     // RUN order (the PCG vector update's r.r, r.z and b.b): the flat blocks'
-    // partials summed sequentially from +0.0 in G = min(blocks, UPD_SLOTS) runs
-    // of consecutive blocks, run c covering blocks [c*nb/G, (c+1)*nb/G); the
-    // run sums combined like partials.
+    // partials summed sequentially from +0.0 in G = min(blocks, UPD_SLOTS) runs,
+    // run c taking blocks c, c+G, c+2G, ... in order; the run sums combined
+    // like partials.
     template <class Term>
     double ureduce(Term term) const {
         const std::vector<double> P = fblocks(term);
@@ -448,7 +448,7 @@ struct Oracle {
         std::vector<double> U(G);
         for (long c = 0; c < G; ++c) {
             double acc = 0.0;
-            for (long b = c * nb / G; b < (c + 1) * nb / G; ++b) acc = acc + P[b];
+            for (long b = c; b < nb; b += G) acc = acc + P[b];
             U[c] = acc;
         }
         return combine(U);
