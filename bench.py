@@ -393,7 +393,9 @@ def main():
     ms_k2 = g.time_kernel(1, reps=20)
     detect = not args.no_detect
     alg_k1 = (40 if detect else 32) * nodes + 16 * elems   # read z, p_old[, w]; write p, Ap; read k, rho*c
-    alg_k2 = 64 * nodes                                     # read x, p, Ap, r, d; write x, r, z
+    # the update at an odd iteration (timed): read x, p_{k-1}, p_k, Ap, r, d; write x, r, z
+    # (an even iteration skips x: read Ap, r, d; write r, z)
+    alg_k2 = 72 * nodes
     peak, peak_kind = peaks()
     ach = alg_k1 / (ms_k1 * 1e-3) / 1e9
     traffic, traffic_src = measure_traffic(N, args) if (world == 1 and args.measure_traffic) else \

@@ -583,8 +583,11 @@ __device__ __forceinline__ void update_scalars(const UpdateArgs& a, const double
         st->rel0 = __ddiv_rn(__dsqrt_rn(part[2]), bnorm);
         st->iter = 0; st->broken = 0; st->result = 0; st->beta = 0.0;
         st->done = (st->max_iter <= 0) ? 1 : 0;
+        st->x_pend = 0;
     } else {
         const int iter = st->iter;
+        st->x_pend = (iter & 1) ? 0 : 1;        // an even iteration leaves its x update owed
+        st->x_pend_iter = iter;
         const double rnorm = __dsqrt_rn(part[0]);
         const double rel = __ddiv_rn(rnorm, st->bnorm);
         const bool conv = rel < st->tol;
@@ -663,6 +666,7 @@ __global__ void __launch_bounds__(RT, kUpdateCtasPerSm) k_update(UpdateArgs a) {
                     if (a.use_cond) cudaGraphSetConditional(a.cond, 0u);
                 } else {
                     st->alpha = __ddiv_rn(st->rho, q[0]);
+                    st->alpha_hist[st->iter & 1] = st->alpha;
                 }
                 s_pAp = q[0];
             }
@@ -677,6 +681,11 @@ __global__ void __launch_bounds__(RT, kUpdateCtasPerSm) k_update(UpdateArgs a) {
         alpha = __ddiv_rn(st->rho, pAp);
     }
     const double nalpha = -alpha;
+    // x += alpha p runs at odd iterations, for the previous iteration and this
+    // one (the previous p is still in the other buffer, its alpha in alpha_hist)
+    const bool xupd = !pre && (iter & 1);
+    const double* p_prev = (iter & 1) ? a.pbuf0 : a.pbuf1;
+    const double alpha_prev = xupd ? st->alpha_hist[(iter - 1) & 1] : 0.0;
     // one flat block: its 3 partials (PRE: bb, rz, rr   LOOP: rr, rz, -) into part
     auto block = [&](long long blk, double* part) {
         const long long m0 = (blk * RT + tid) * KF;
@@ -718,12 +727,21 @@ __global__ void __launch_bounds__(RT, kUpdateCtasPerSm) k_update(UpdateArgs a) {
             }
             stv(a.r, r_); stv(a.z, z_);
         } else {
-            double xx[KF], pp[KF], qq[KF], rr[KF], dd[KF];
-            ld(a.x, xx); ld(p, pp); ld(a.Ap, qq); ld(a.r, rr); ld(a.d, dd);
+            double qq[KF], rr[KF], dd[KF];
+            ld(a.Ap, qq); ld(a.r, rr); ld(a.d, dd);
+            if (xupd) {
+                // x += alpha_{k-1} p_{k-1}, then x += alpha_k p_k: the same two
+                // multiply-adds, in the same order, as one update per iteration
+                double xx[KF], pp[KF], po[KF];
+                ld(a.x, xx); ld(p_prev, po); ld(p, pp);
+#pragma unroll
+                for (int k = 0; k < KF; ++k)
+                    if (has(k)) xx[k] = dfma(alpha, pp[k], dfma(alpha_prev, po[k], xx[k]));
+                stv(a.x, xx);
+            }
 #pragma unroll
             for (int k = 0; k < KF; ++k) {
                 if (!has(k)) continue;
-                xx[k] = dfma(alpha, pp[k], xx[k]);
                 double rk = dfma(nalpha, qq[k], rr[k]);
                 if (fi_r && m0 + k == fi_idx) rk = flipbit(rk, fi_bit);
                 rr[k] = rk;
@@ -731,7 +749,7 @@ __global__ void __launch_bounds__(RT, kUpdateCtasPerSm) k_update(UpdateArgs a) {
                 part[0] = dfma(rk, rk, part[0]);
                 part[1] = dfma(rk, dd[k], part[1]);
             }
-            stv(a.x, xx); stv(a.r, rr); stv(a.z, dd);
+            stv(a.r, rr); stv(a.z, dd);
         }
     };
     // run blockIdx.x of the RUN order: flat blocks c, c+G, ..., their partials
@@ -765,6 +783,18 @@ __global__ void __launch_bounds__(RT, kUpdateCtasPerSm) k_update(UpdateArgs a) {
         *a.ticket = 0u;
         update_scalars(a, v);
     }
+}
+
+// The solution update still owed when the PCG loop ends (its last update ran
+// at an even iteration): x += alpha p of that iteration.
+__global__ void __launch_bounds__(RT) k_update_finish(long long Nn, double* x, const double* pbuf0,
+                                                     const double* pbuf1, const DevState* st) {
+    if (!st->x_pend) return;
+    const int k = st->x_pend_iter;
+    const double* p = (k & 1) ? pbuf1 : pbuf0;
+    const double alpha = st->alpha_hist[k & 1];
+    for (long long i = (long long)blockIdx.x * RT + threadIdx.x; i < Nn; i += (long long)gridDim.x * RT)
+        x[i] = dfma(alpha, p[i], x[i]);
 }
 
 // ---- generic reductions over node vectors (canonical partition) ---------------

@@ -256,6 +256,11 @@ void launch_update(hs_solver* h, int role, bool use_cond, cudaGraphConditionalHa
     launch_k(pdl, k_update, (int)std::min<long long>(h->part.nflat, UPD_SLOTS), RT, 0, h->s, u);
 }
 
+// the solution update the loop still owes (x += alpha p of an even last iteration)
+void launch_update_finish(hs_solver* h) {
+    k_update_finish<<<grid_for(h->Nn, RT), RT, 0, h->s>>>(h->Nn, h->T.p, h->p0.p, h->p1.p, h->st.p);
+}
+
 void launch_reduce(hs_solver* h, int kind, const double* a, const double* b, double* out) {
     RedArgs r{h->Nn, h->part.nflat, h->N, kind, a, b, h->partials.p, h->ticket.p, out};
     k_reduce<<<(int)h->part.nflat, RT, 0, h->s>>>(r);
@@ -337,6 +342,14 @@ hs_status build_graph(hs_solver* h, int which) {
         launch_update(h, UPD_LOOP, true, cond, pdl);
     }
     HS_CUDA(cudaStreamEndCapture(h->s, &body));
+    // after the loop: the solution update still owed
+    cudaGraph_t post;
+    HS_CUDA(cudaStreamBeginCapture(h->s, cudaStreamCaptureModeThreadLocal));
+    launch_update_finish(h);
+    HS_CUDA(cudaStreamEndCapture(h->s, &post));
+    cudaGraphNode_t n_post;
+    HS_CUDA(cudaGraphAddChildGraphNode(&n_post, g, &n_loop, 1, post));
+    cudaGraphDestroy(post);
     HS_CUDA(cudaGraphInstantiate(&h->gexec[which], g, 0));
     h->graph[which] = g;
     return HS_OK;
@@ -667,6 +680,7 @@ hs_status pcg_direct(hs_solver* h, bool with_rhs) {
         HS_CUDA(cudaStreamSynchronize(h->s));
         if (hsx.done) break;
     }
+    launch_update_finish(h);
     HS_CUDA(cudaGetLastError());
     return HS_OK;
 }

@@ -117,6 +117,11 @@ struct DevState {
     double* log_alpha;
     double* log_beta;
     int log_cap, pad1;
+    // the solution update x += alpha_k p_k runs every second CG iteration: at
+    // an odd k for k-1 and k (alpha_hist[k & 1] holds alpha_k); x_pend marks a
+    // last update (at x_pend_iter) still owed when the loop ends
+    double alpha_hist[2];
+    int x_pend, x_pend_iter;
     // scratch outputs of standalone reductions
     double red_out[MAXQ];
     double mm_out[2];       // min, max
