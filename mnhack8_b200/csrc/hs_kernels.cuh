@@ -614,9 +614,10 @@ __device__ __forceinline__ void update_scalars(const UpdateArgs& a, const double
 // checksum and a breakdown.
 //
 // It also finishes its own reductions, in the RUN order: CTA c of the
-// G = min(nflat, UPD_SLOTS) CTAs takes the flat blocks c, c+G, c+2G, ... in
-// order and sums their block partials, and
-// the last CTA to finish (an atomic ticket) combines the G run sums
+// G = min(nflat, UPD_SLOTS) CTAs takes the flat blocks c, c+G, c+2G, ..., each
+// thread carrying one sum through its nodes of all of them, reduces the run
+// with one block tree, and the last CTA to finish (an atomic ticket) combines
+// the G run sums
 // (final_sums) and runs the scalar logic, the work a separate single-CTA
 // kernel would do after it.  G fits one resident wave (5 CTAs per SM), so the
 // last CTA's pass reads at most UPD_SLOTS partials per quantity.
@@ -627,7 +628,6 @@ __global__ void __launch_bounds__(RT, kUpdateCtasPerSm) k_update(UpdateArgs a) {
     constexpr int NC = KF / 2;
     __shared__ double sh[MAXQ][8];
     __shared__ double s_pAp;
-    __shared__ double s_run[3];
     __shared__ unsigned s_last;
     DevState* st = a.st;
     const int tid = threadIdx.x;
@@ -752,23 +752,16 @@ __global__ void __launch_bounds__(RT, kUpdateCtasPerSm) k_update(UpdateArgs a) {
             stv(a.r, rr); stv(a.z, dd);
         }
     };
-    // run blockIdx.x of the RUN order: flat blocks c, c+G, ..., their partials
-    // summed in order from +0.0 (the running sums live in shared memory,
-    // written by thread 0 only)
+    // run blockIdx.x of the RUN order: flat blocks c, c+G, ...; each thread
+    // carries one sum through its nodes of all the run's blocks, and the run
+    // takes one block tree at the end
     const int G = gridDim.x, c = blockIdx.x;
-    if (tid == 0) { s_run[0] = 0.0; s_run[1] = 0.0; s_run[2] = 0.0; }
-    for (int blk = c; blk < a.nflat; blk += G) {
-        double part[3] = {0.0, 0.0, 0.0};
-        block(blk, part);
-        cta_tree_sum<3>(part, sh);
-        if (tid == 0) {
-#pragma unroll
-            for (int q = 0; q < 3; ++q) s_run[q] = dadd(s_run[q], part[q]);
-        }
-    }
+    double part[3] = {0.0, 0.0, 0.0};
+    for (int blk = c; blk < a.nflat; blk += G) block(blk, part);
+    cta_tree_sum<3>(part, sh);
     if (tid == 0) {
 #pragma unroll
-        for (int q = 0; q < 3; ++q) a.partials[(long long)q * G + c] = s_run[q];
+        for (int q = 0; q < 3; ++q) a.partials[(long long)q * G + c] = part[q];
         __threadfence();
         const unsigned t = atomicAdd(a.ticket, 1u);
         s_last = (t == gridDim.x - 1) ? 1u : 0u;

@@ -17,10 +17,11 @@ namespace hs {
 // FLAT partition (the other reductions and the PCG vector update): blocks of
 // RT*KF consecutive nodes, thread t of block b taking the KF consecutive nodes
 // b*RT*KF + t*KF + k.
-// RUN order (the PCG vector update's b.b, r.z and r.r): the FLAT blocks'
-// partials summed sequentially from +0.0 in G = min(blocks, UPD_SLOTS) runs,
-// run c taking blocks c, c+G, c+2G, ... in order; the run sums are then
-// combined like per-block partials.
+// RUN order (the PCG vector update's b.b, r.z and r.r): the FLAT blocks are
+// dealt to G = min(blocks, UPD_SLOTS) runs, run c taking blocks c, c+G, ...;
+// thread t of a run accumulates its KF nodes of each of the run's blocks,
+// block after block, in one sum; the run's RT sums go through the block tree
+// and the G run sums are then combined like per-block partials.
 // In all, a block combines its RT values by a 32-lane xor butterfly per warp
 // and an 8-way xor butterfly over the warp sums, and a final pass combines the
 // per-block partials by RT strided sequential sums and the same block tree.

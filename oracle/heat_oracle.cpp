@@ -436,20 +436,32 @@ struct Oracle {
     }
     template <class Term>
     double freduce(Term term) const { return combine(fblocks(term)); }
-    // RUN order (the PCG vector update's r.r, r.z and b.b): the flat blocks'
-    // partials summed sequentially from +0.0 in G = min(blocks, UPD_SLOTS) runs,
-    // run c taking blocks c, c+G, c+2G, ... in order; the run sums combined
-    // like partials.
+    // RUN order (the PCG vector update's r.r, r.z and b.b): the flat blocks
+    // (RT*KF consecutive nodes) are dealt to G = min(blocks, UPD_SLOTS) runs,
+    // run c taking blocks c, c+G, c+2G, ...; thread t of a run accumulates its
+    // KF nodes of each of the run's blocks, block after block, in one sum from
+    // +0.0; the run's RT sums go through the block tree, and the G run sums
+    // are combined like partials.
     template <class Term>
     double ureduce(Term term) const {
-        const std::vector<double> P = fblocks(term);
-        const long nb = (long)P.size();
+        const long RB = (long)RT * g_KF;
+        const long nb = (Nn + RB - 1) / RB;
         const long G = nb < UPD_SLOTS ? nb : UPD_SLOTS;
         std::vector<double> U(G);
+        #pragma omp parallel for schedule(static)
         for (long c = 0; c < G; ++c) {
-            double acc = 0.0;
-            for (long b = c; b < nb; b += G) acc = acc + P[b];
-            U[c] = acc;
+            double v[RT];
+            for (int l = 0; l < RT; ++l) {
+                double acc = 0.0;
+                for (long b = c; b < nb; b += G)
+                    for (int k = 0; k < g_KF; ++k) {
+                        const long n = b * RB + (long)l * g_KF + k;
+                        if (n >= Nn) break;
+                        acc = term(n, acc);
+                    }
+                v[l] = acc;
+            }
+            U[c] = tree256(v);
         }
         return combine(U);
     }
