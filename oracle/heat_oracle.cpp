@@ -730,6 +730,8 @@ double or_apply(void* h, const double* x, double* y, double dt_eff, int project,
 }
 
 double or_dot(void* h, const double* a, const double* b) { return ((Oracle*)h)->dot(a, b); }
+// the PCG update's order (RUN)
+double or_udot(void* h, const double* a, const double* b) { return ((Oracle*)h)->udot(a, b); }
 
 void or_build_rhs(void* h, const double* T, double* b) { ((Oracle*)h)->build_rhs(T, b); }
 

@@ -50,6 +50,8 @@ def lib():
         L.or_apply.argtypes = [vp, dp, dp, C.c_double, C.c_int, C.c_int, C.c_long, C.c_int]
         L.or_dot.restype = C.c_double
         L.or_dot.argtypes = [vp, dp, dp]
+        L.or_udot.restype = C.c_double
+        L.or_udot.argtypes = [vp, dp, dp]
         L.or_build_rhs.argtypes = [vp, dp, dp]
         L.or_pcg.restype = C.c_int
         L.or_pcg.argtypes = [vp, dp, dp, C.c_int, C.c_double, vp, vp, vp, vp]
@@ -151,6 +153,11 @@ class Oracle:
     def dot(self, a, b):
         return lib().or_dot(self._h, np.ascontiguousarray(a, dtype=np.float64),
                             np.ascontiguousarray(b, dtype=np.float64))
+
+    def udot(self, a, b):
+        """x.y in the PCG update's RUN order."""
+        return lib().or_udot(self._h, np.ascontiguousarray(a, dtype=np.float64),
+                             np.ascontiguousarray(b, dtype=np.float64))
 
     def build_rhs(self, T):
         b = np.zeros(self.Nn)
