@@ -402,14 +402,15 @@ def main():
         (None, "not measured in this run (a 1-GPU bench.py --measure-traffic takes it)")
     iters_per_traj = it_all / max(1, world) / args.steps
     # per time step: step begin/end, RHS and x0 operator (+ their final kernel with
-    # ABFT), the PCG prologue's update; per CG iteration: operator and update (whose
-    # last CTA finishes the reductions); the graph's while body runs 4 iterations
-    # per pass, so a step launches whole passes.  The atomic scatter adds p
-    # formation, zeroing and the finishing pass to each operator.
+    # ABFT), the PCG prologue's update, the solution update owed after the loop;
+    # per CG iteration: operator and update (whose last CTA finishes the
+    # reductions); the graph's while body runs 4 iterations per pass, so a step
+    # launches whole passes.  The atomic scatter adds p formation, zeroing and
+    # the finishing pass to each operator.
     if args.scatter == "colored":
-        per_step, per_iter = 2 + 2 * (2 if detect else 1) + 1, 2
+        per_step, per_iter = 2 + 2 * (2 if detect else 1) + 2, 2
     else:
-        per_step, per_iter = 2 + 2 * (4 if detect else 3) + 1, 5
+        per_step, per_iter = 2 + 2 * (4 if detect else 3) + 2, 5
     it_step = iters_per_traj / STEPS_PER_TRAJ
     loop_iters = 4 * int(np.ceil(it_step / 4))
     launches = int(round(args.steps * STEPS_PER_TRAJ * (per_step + per_iter * loop_iters)))
