@@ -413,7 +413,10 @@ __device__ __forceinline__ void slab_march(const ApplyArgs& a, SlabSmem& S, cons
         if (ix >= 0 && ix < N) {
 #pragma unroll
             for (int k = 0; k < SK; ++k) {
-                if (!sp_elem(fl, k)) continue;
+                // every position computes its element (zero coefficients where there
+                // is none), so the SK elements carry no branch between them; only the
+                // hand-over stores are guarded
+                const bool ev = sp_elem(fl, k);
                 const int j = tid + k * ST;
                 double v[8];
                 v[0] = pc[k];
@@ -428,9 +431,11 @@ __device__ __forceinline__ void slab_march(const ApplyArgs& a, SlabSmem& S, cons
                 if (fi_r && (long long)ix * eplane + G.eoff[k] == fi_elem) v[0] = flipbit(v[0], fi_bit);
                 ac[k] = dadd(ac[k], v[0]);
                 an[k] = dadd(0.0, v[4]);
-                S.Y1[j + 1] = make_double2(v[1], v[5]);
-                S.Y2[j + Cw] = make_double2(v[2], v[6]);
-                S.Y3[j + Cw + 1] = make_double2(v[3], v[7]);
+                if (ev) {
+                    S.Y1[j + 1] = make_double2(v[1], v[5]);
+                    S.Y2[j + Cw] = make_double2(v[2], v[6]);
+                    S.Y3[j + Cw + 1] = make_double2(v[3], v[7]);
+                }
             }
         }
         ld_coef(ix + 1 <= xb ? ix + 1 : -1);
