@@ -479,7 +479,7 @@ def serving_leg(n, device):
     from mnhack8_b200 import ensemble
     r = ensemble.serving(n=n, device=device)
     return {"requests": n, "stream": "Poisson 200/s, N 16..160, steps 10..100, 30% one bit flip, rtol 1e-8",
-            "stream_span_s": r["stream_span_s"], "peak_live": r["peak_live"],
+            "stream_span_s": r["stream_span_s"], "max_live": r["max_live"], "peak_live": r["peak_live"],
             "batched": r["batched"], "serial_fp64": r["serial_fp64"], "solves_per_s_ratio": r["throughput_ratio"],
             "field_generation": r["field_generation"]}
 

@@ -202,12 +202,13 @@ def request_stream(n, rate, seed, nmin=16, nmax=160, smin=10, smax=100, flip_fra
     return reqs
 
 
-def serving(n=400, rate=200.0, seed=11, rtol=1e-8, inner_tol=1e-4, max_live=64, hbm_fraction=0.5, device=0,
-            gpu_fields=False):
+def serving(n=400, rate=200.0, seed=11, rtol=1e-8, inner_tol=1e-4, max_live=256, hbm_fraction=0.5, device=0,
+            gpu_fields=False, serial=True):
     """gpu_fields: the batched server generates each request's field on the
     device when it admits the request (hs_batch_add_lognormal), so the field's
     generation is inside the served latency; the serial FP64 side keeps the
-    host fields generated before its timed region."""
+    host fields generated before its timed region.  serial=False times the
+    batched server alone."""
     import torch
     import concurrent.futures as cf
     import multiprocessing as mp
@@ -273,6 +274,11 @@ def serving(n=400, rate=200.0, seed=11, rtol=1e-8, inner_tol=1e-4, max_live=64, 
             b.remove(s)
     wall_b = time.perf_counter() - t0
     b.close()
+    if not serial:
+        return {"form": "serving", "requests": n, "max_live": max_live, "peak_live": peak_live,
+                "batched": {"wall_s": wall_b, "solves_per_s": n / wall_b,
+                            "p50_latency_s": float(np.percentile(list(lat.values()), 50)),
+                            "p99_latency_s": float(np.percentile(list(lat.values()), 99))}}
     # serial plain FP64: the same stream, one solve at a time
     lat_s = {}
     create_s = 0.0
@@ -528,7 +534,7 @@ def _main(argv=None):
     p.add_argument("--gpu-fields", action="store_true")
     p.add_argument("--n", type=int, default=400)
     p.add_argument("--rate", type=float, default=200.0)
-    p.add_argument("--max-live", type=int, default=64)
+    p.add_argument("--max-live", type=int, default=256)
     a = ap.parse_args(argv)
     if a.cmd == "precision":
         out = precision(N=a.N, steps=a.steps)
