@@ -574,7 +574,7 @@ struct UpdateArgs {
     long long nblk;             // LOOP: their count per quantity
 };
 
-// PCG scalar logic after the vector update, on the FLAT-order sums: the
+// PCG scalar logic after the vector update, on the RUN-order sums: the
 // prologue's ||b||, rho and initial residual, or the loop's convergence test
 // (||r||/||b|| < tol, the reference's recursive residual), beta = rho_new /
 // rho and the iteration count; sets the graph's while condition.

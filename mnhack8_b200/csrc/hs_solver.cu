@@ -85,7 +85,7 @@ struct hs_solver {
     DevBuf<double> diag, F, wM, wA;
     DevBuf<double> T, b, r, z, p0, p1, Ap;
     DevBuf<double> partials;            // operator tiles (and the standalone reductions)
-    DevBuf<double> upart;               // PCG vector update: per-block partials (FLAT order)
+    DevBuf<double> upart;               // PCG vector update: run sums (RUN order)
     int n_sm = 148;
     DevBuf<unsigned> ticket;
     DevBuf<DevState> st;
