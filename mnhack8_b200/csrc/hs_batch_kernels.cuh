@@ -374,8 +374,18 @@ __device__ __forceinline__ void kb_tile(const BatchArgs& B, BSlabSmem<V>& S, lon
         for (int k = 0; k < SK; ++k) { pA[k] = pB[k]; aA[k] = aB[k]; }
     }
     if (!loop && !d1) return;
-    cta_tree_csum<MAXQ>(part, S.sh);
-    if (threadIdx.x == 0) store_cpartials<MAXQ>(part, B.pa, B.ntiles, t);
+    if constexpr (sizeof(V) == 8) {
+        cta_tree_csum<MAXQ>(part, S.sh);
+        if (threadIdx.x == 0) store_cpartials<MAXQ>(part, B.pa, B.ntiles, t);
+    } else {
+        // FP32 applies: plain FP64 sums, stored with lo = 0 in the same layout
+        double ph[MAXQ] = {part[0].hi, part[1].hi, part[2].hi, part[3].hi};
+        cta_tree_sum<MAXQ>(ph, S.sh);
+        if (threadIdx.x == 0) {
+            const CSum pc[MAXQ] = {{ph[0], 0.0}, {ph[1], 0.0}, {ph[2], 0.0}, {ph[3], 0.0}};
+            store_cpartials<MAXQ>(pc, B.pa, B.ntiles, t);
+        }
+    }
 }
 
 template <typename V, int KIND>
@@ -427,6 +437,33 @@ __device__ __forceinline__ void inst_sums(double (&v)[NQ], const double* base, l
     for (int q = 0; q < NQ; ++q) v[q] = csum_value(acc[q]);
 }
 
+// plain sums of one instance's partials whose lo parts are zero (the FP32
+// inner solve's): hi of quantity q at base + q*qstride; RT strided sequential
+// sums, then the block tree; valid in thread 0
+template <int NQ>
+__device__ __forceinline__ void inst_sums_plain(double (&v)[NQ], const double* base, long long count,
+                                                long long qstride, double (*sh)[8]) {
+    constexpr int FB = 8;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) v[q] = 0.0;
+    for (long long k0 = threadIdx.x; k0 < count; k0 += (long long)RT * FB) {
+        double th[NQ][FB];
+#pragma unroll
+        for (int q = 0; q < NQ; ++q)
+#pragma unroll
+            for (int u = 0; u < FB; ++u) {
+                const long long k = k0 + (long long)u * RT;
+                th[q][u] = (k < count) ? __ldcg(base + q * qstride + k) : 0.0;
+            }
+#pragma unroll
+        for (int q = 0; q < NQ; ++q)
+#pragma unroll
+            for (int u = 0; u < FB; ++u)
+                if (k0 + (long long)u * RT < count) v[q] = dadd(v[q], th[q][u]);
+    }
+    cta_tree_sum<NQ>(v, sh);
+}
+
 __device__ __forceinline__ double d1_rel(const double (&p)[MAXQ], double nw) {
     const double nx = __dsqrt_rn(p[3]);
     double rel = __ddiv_rn(fabs(dsub(p[1], p[2])), dfma(nw, nx, 1e-300));
@@ -446,7 +483,8 @@ __global__ void __launch_bounds__(RT) kb_final_apply(BatchArgs B) {
     if (KIND == BK_LOOP && (st->odone || st->done)) return;
     if (KIND == BK_RESID && st->odone) return;
     double p[MAXQ];
-    inst_sums<MAXQ>(p, B.pa + I.tile0, I.part.ntiles, B.ntiles, sh);
+    if (KIND == BK_LOOP) inst_sums_plain<MAXQ>(p, B.pa + I.tile0, I.part.ntiles, B.ntiles, sh);
+    else inst_sums<MAXQ>(p, B.pa + I.tile0, I.part.ntiles, B.ntiles, sh);
     if (threadIdx.x != 0) return;
     if (B.detect) {
         const double rel = d1_rel(p, KIND == BK_RHS ? st->norm_wM : st->norm_wA);
@@ -599,8 +637,14 @@ __global__ void __launch_bounds__(RT) kb_update32(BatchArgs B) {
             }
         }
     }
-    cta_tree_csum<2>(part, sh);
-    if (threadIdx.x == 0 && blockIdx.x < B.nflat) store_cpartials<2>(part, B.pf, B.nflat, blockIdx.x);
+    // plain FP64 block tree (the inner sums carry no compensation); the
+    // partials keep the (hi, lo) layout of the compensated ones, lo = 0
+    double ph[2] = {part[0].hi, part[1].hi};
+    cta_tree_sum<2>(ph, sh);
+    if (threadIdx.x == 0 && blockIdx.x < B.nflat) {
+        const CSum pc[2] = {{ph[0], 0.0}, {ph[1], 0.0}};
+        store_cpartials<2>(pc, B.pf, B.nflat, blockIdx.x);
+    }
 }
 
 // one block per instance: inner convergence and beta
@@ -613,7 +657,7 @@ __global__ void __launch_bounds__(RT) kb_final_update32(BatchArgs B) {
     BState* st = I.st;
     if (st->odone || st->done) return;
     double p[2];
-    inst_sums<2>(p, B.pf + I.flat0, I.part.nflat, B.nflat, sh);
+    inst_sums_plain<2>(p, B.pf + I.flat0, I.part.nflat, B.nflat, sh);
     if (threadIdx.x != 0) return;
     st->inner_total += 1;
     const double rel = __ddiv_rn(__dsqrt_rn(p[0]), st->bn_in);
