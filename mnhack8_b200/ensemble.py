@@ -158,7 +158,7 @@ def batching(n=256, nmin=16, nmax=96, steps=20, rtol=1e-8, inner_tol=1e-4, seed=
     fields = [(N, k, r, _lib.gaussian_ic(N, IC_SIGMA)) for (N, _), (k, r) in zip(specs, kr)]
     # autotuner: planes per operator tile (0: the per-N default), timed on 2 steps of the first 64 instances
     tune = {}
-    for planes in (0, 8, 16, 32):
+    for planes in (0, 8, 12, 16, 24, 32):
         run_batch(fields[:64], 1, rtol, inner_tol, planes, device)         # capture / warm
         ms, _ = run_batch(fields[:64], 2, rtol, inner_tol, planes, device)
         tune[planes] = ms
